@@ -1,0 +1,202 @@
+"""ctypes mirror of include/pdeb200.h and the loader for libpdeb200.so.
+
+The structures here must stay byte-identical to the C header; tests check
+their sizes against the library's own sizeof values (pdeb200_sizeof_*).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PDEB200_ABI_VERSION = 1
+
+# pdeb200_status
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_CUDA, ERR_OOM = 0, 1, 2, 3, 4, 5
+ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_DEGENERATE, ERR_CANCELLED, ERR_TIMEOUT, ERR_BUSY = 6, 7, 8, 9, 10, 11
+
+# boundary kinds (BCKind order)
+BC_DIRICHLET, BC_NEUMANN, BC_ROBIN = 0, 1, 2
+# coefficient forms
+COEF_CONST, COEF_DIVK, COEF_NODAL = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+# methods (SolveMethod order, then the B200 forms)
+JACOBI, GAUSS_SEIDEL, SOR, CG, BICGSTAB, GMRES, MG_VCYCLE, MG_PCG, MG_BICGSTAB = range(9)
+TOL_REFERENCE, TOL_RELATIVE = 0, 1
+FP64, MIXED = 0, 1
+ORDER_LEXICOGRAPHIC, ORDER_REDBLACK = 0, 1
+
+FACE_NAMES = ("left", "right", "bottom", "top", "front", "back")
+
+
+class Face(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("reserved", C.c_int32),
+        ("value", C.c_double),
+        ("alpha", C.c_double),
+        ("beta", C.c_double),
+        ("gamma", C.c_double),
+        ("value_arr", C.POINTER(C.c_double)),
+        ("alpha_arr", C.POINTER(C.c_double)),
+        ("beta_arr", C.POINTER(C.c_double)),
+        ("gamma_arr", C.POINTER(C.c_double)),
+    ]
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("coef_kind", C.c_int32),
+        ("mem_space", C.c_int32),
+        ("reserved", C.c_int32),
+        ("xmin", C.c_double),
+        ("xmax", C.c_double),
+        ("ymin", C.c_double),
+        ("ymax", C.c_double),
+        ("zmin", C.c_double),
+        ("zmax", C.c_double),
+        ("a", C.c_double),
+        ("b", C.c_double),
+        ("az", C.c_double),
+        ("c", C.c_double),
+        ("d", C.c_double),
+        ("dz", C.c_double),
+        ("e", C.c_double),
+        ("f_const", C.c_double),
+        ("ut", C.c_double),
+        ("k", C.POINTER(C.c_double)),
+        ("nodal", C.POINTER(C.c_double)),
+        ("f", C.POINTER(C.c_double)),
+        ("u0", C.POINTER(C.c_double)),
+        ("face", Face * 6),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("method", C.c_int32),
+        ("max_iter", C.c_int32),
+        ("tol", C.c_double),
+        ("tol_mode", C.c_int32),
+        ("precision", C.c_int32),
+        ("sor_omega", C.c_double),
+        ("gmres_restart", C.c_int32),
+        ("mg_pre_smooth", C.c_int32),
+        ("mg_post_smooth", C.c_int32),
+        ("mg_coarse_iters", C.c_int32),
+        ("mg_max_levels", C.c_int32),
+        ("gs_ordering", C.c_int32),
+        ("device", C.c_int32),
+        ("check_interval", C.c_int32),
+        ("inner_tol", C.c_double),
+        ("bf16_coefficients", C.c_int32),
+        ("max_outer", C.c_int32),
+        ("cancel", C.POINTER(C.c_int32)),
+    ]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("outer_iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("kernel_launches", C.c_int32),
+        ("residual_l2", C.c_double),
+        ("rhs_l2", C.c_double),
+        ("rel_residual", C.c_double),
+        ("last_delta", C.c_double),
+        ("device_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("message", C.c_char * 256),
+    ]
+
+
+class TimeOptions(C.Structure):
+    _fields_ = [
+        ("t_start", C.c_double),
+        ("dt", C.c_double),
+        ("frames", C.c_int32),
+        ("frame_stride", C.c_int32),
+        ("device", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class ProjectionOptions(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32),
+        ("fix_pressure_corner", C.c_int32),
+        ("tol", C.c_double),
+        ("reference_pressure", C.c_double),
+        ("device", C.c_int32),
+        ("mem_space", C.c_int32),
+    ]
+
+
+class ProjectionReport(C.Structure):
+    _fields_ = [
+        ("success", C.c_int32),
+        ("poisson_iterations", C.c_int32),
+        ("poisson_residual", C.c_double),
+        ("max_divergence_before", C.c_double),
+        ("max_divergence_after", C.c_double),
+        ("l2_divergence_before", C.c_double),
+        ("l2_divergence_after", C.c_double),
+        ("device_ms", C.c_double),
+        ("message", C.c_char * 256),
+    ]
+
+
+FRAME_CB = C.CFUNCTYPE(C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_void_p)
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libpdeb200.so")
+
+_LIB = None
+
+
+def declare(lib: C.CDLL) -> C.CDLL:
+    """Attach argtypes/restype of every exported entry point."""
+    P = C.POINTER
+    lib.pdeb200_abi_version.restype = C.c_int32
+    lib.pdeb200_abi_version.argtypes = []
+    lib.pdeb200_probe.restype = C.c_int32
+    lib.pdeb200_probe.argtypes = [C.c_char_p, C.c_size_t]
+    lib.pdeb200_status_string.restype = C.c_char_p
+    lib.pdeb200_status_string.argtypes = [C.c_int32]
+    lib.pdeb200_default_options.restype = None
+    lib.pdeb200_default_options.argtypes = [P(Options)]
+    lib.pdeb200_release_all.restype = None
+    lib.pdeb200_release_all.argtypes = []
+    lib.pdeb200_solve.restype = C.c_int32
+    lib.pdeb200_solve.argtypes = [P(Problem), P(Options), C.c_void_p, P(Report)]
+    lib.pdeb200_residual_norms.restype = C.c_int32
+    lib.pdeb200_residual_norms.argtypes = [P(Problem), C.c_void_p, C.c_int32, P(C.c_double), P(C.c_double)]
+    lib.pdeb200_apply.restype = C.c_int32
+    lib.pdeb200_apply.argtypes = [P(Problem), C.c_void_p, C.c_void_p, C.c_int32]
+    lib.pdeb200_time_series.restype = C.c_int32
+    lib.pdeb200_time_series.argtypes = [P(Problem), P(TimeOptions), FRAME_CB, C.c_void_p, C.c_void_p, P(Report)]
+    lib.pdeb200_project_velocity.restype = C.c_int32
+    lib.pdeb200_project_velocity.argtypes = [
+        C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(ProjectionOptions), P(ProjectionReport)]
+    return lib
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Load libpdeb200.so. Raises if the library has not been built: there is
+    no fallback implementation."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"libpdeb200.so not built at {p}; run __graft_entry__.build()")
+    lib = declare(C.CDLL(p))
+    if lib.pdeb200_abi_version() != PDEB200_ABI_VERSION:
+        raise RuntimeError("libpdeb200.so ABI version mismatch")
+    if path is None:
+        _LIB = lib
+    return lib
