@@ -59,6 +59,8 @@ def restate() -> C.CDLL:
         lib.rs_folded_apply.argtypes = [P(abi.Problem), DP, DP]
         lib.rs_fill_boundary.restype = C.c_int
         lib.rs_fill_boundary.argtypes = [P(abi.Problem), DP]
+        lib.rs_sizeof.restype = C.c_long
+        lib.rs_sizeof.argtypes = [C.c_int]
         lib.rs_set_threads.restype = None
         lib.rs_set_threads.argtypes = [C.c_int]
         _restate = lib

@@ -1596,3 +1596,18 @@ int rs_project(int nx, int ny, int nz, double dx, double dy, double dz, double d
   free(Ap);
   return ok ? PDEB200_OK : PDEB200_ERR_NOT_CONVERGED;
 }
+
+/* sizeof of the ABI structs as compiled by a C compiler from include/pdeb200.h
+ * (tests compare them with the ctypes mirror). */
+long rs_sizeof(int which) {
+  switch (which) {
+    case 0: return (long)sizeof(pdeb200_face);
+    case 1: return (long)sizeof(pdeb200_problem);
+    case 2: return (long)sizeof(pdeb200_options);
+    case 3: return (long)sizeof(pdeb200_report);
+    case 4: return (long)sizeof(pdeb200_time_options);
+    case 5: return (long)sizeof(pdeb200_projection_options);
+    case 6: return (long)sizeof(pdeb200_projection_report);
+    default: return -1;
+  }
+}

@@ -31,6 +31,7 @@ int rs_folded_rhs(const pdeb200_problem* prob, double* b);
 int rs_folded_apply(const pdeb200_problem* prob, const double* x, double* y);
 int rs_fill_boundary(const pdeb200_problem* prob, double* grid);
 void rs_set_threads(int n);
+long rs_sizeof(int which);
 
 #ifdef __cplusplus
 }

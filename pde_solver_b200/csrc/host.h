@@ -1,0 +1,168 @@
+// Host-side runtime of libpdeb200: per-device contexts, stream-ordered device
+// buffers, the device copy of a problem and the launch helpers shared by the
+// solver drivers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pdeb200.h"
+#include "kernels.cuh"
+
+namespace pdeb {
+
+struct Error {
+  pdeb200_status status = PDEB200_OK;
+  std::string msg;
+};
+
+#define PDEB_CUDA(call)                                                         \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) throw CudaFailure(e_, #call, __FILE__, __LINE__);    \
+  } while (0)
+
+struct CudaFailure {
+  cudaError_t err;
+  std::string what;
+  CudaFailure(cudaError_t e, const char* call, const char* file, int line)
+      : err(e), what(std::string(cudaGetErrorString(e)) + " at " + file + ":" + std::to_string(line) + " (" + call + ")") {}
+};
+
+struct StatusFailure {
+  pdeb200_status status;
+  std::string what;
+};
+
+// Device buffer from the device's stream-ordered memory pool. The pool keeps
+// freed blocks (release threshold = max), so repeated solves of one shape do
+// not go back to the driver.
+class Buf {
+ public:
+  Buf() = default;
+  Buf(size_t bytes, cudaStream_t s) : bytes_(bytes), s_(s) {
+    if (bytes) {
+      cudaError_t e = cudaMallocAsync(&p_, bytes, s);
+      if (e == cudaErrorMemoryAllocation) throw StatusFailure{PDEB200_ERR_OOM, "device memory exhausted"};
+      PDEB_CUDA(e);
+    }
+  }
+  ~Buf() { reset(); }
+  Buf(const Buf&) = delete;
+  Buf& operator=(const Buf&) = delete;
+  Buf(Buf&& o) noexcept { *this = std::move(o); }
+  Buf& operator=(Buf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p_ = o.p_;
+      bytes_ = o.bytes_;
+      s_ = o.s_;
+      o.p_ = nullptr;
+      o.bytes_ = 0;
+    }
+    return *this;
+  }
+  void reset() {
+    if (p_) cudaFreeAsync(p_, s_);
+    p_ = nullptr;
+    bytes_ = 0;
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p_); }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t bytes_ = 0;
+  cudaStream_t s_ = nullptr;
+};
+
+struct Context {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Ctl* d_ctl = nullptr;     // device control block
+  Ctl* h_ctl = nullptr;     // pinned mirror
+  double* d_partials = nullptr;
+  unsigned* d_tickets = nullptr;
+  double* d_redout = nullptr;
+  size_t max_blocks = 0;
+  int num_sms = 148;
+  std::string name;
+  std::mutex mu;
+  long long launches = 0;
+
+  RedSlot slot(int which = 0) const {
+    return RedSlot{d_partials + (size_t)which * max_blocks * kMaxRed, d_tickets + which, d_redout + which * kMaxRed};
+  }
+  void count(int n = 1) { launches += n; }
+};
+
+Context* get_context(int dev);  // throws StatusFailure / CudaFailure
+void release_contexts();
+
+// Device copy of a problem, with face closures materialised.
+struct DevProblem {
+  GridDev g{};
+  int coef_kind = 0;
+  CoefConst cc{};
+  CoefDivk<double> cd{};
+  CoefNodal cn{};
+  const double* f = nullptr;
+  double f_const = 0.0;
+  const double* u0 = nullptr;
+  double dx = 0, dy = 0, dz = 0;
+  double a = 0, b = 0, az = 0, c = 0, d = 0, dzc = 0, e = 0, ut = 0;
+  std::vector<Buf> owned;
+  bool device_inputs = false;
+};
+
+// Validates and uploads; host arrays of the problem are copied on ctx->stream.
+void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* out);
+
+// Builds the face parameters of `g` for spacing (dx,dy,dz) from the host face
+// descriptions; arrays are sampled with `stride` (1 on the finest level, 2^l
+// on level l) and uploaded into `owned`.
+void build_faces(Context* ctx, const pdeb200_problem* p, int nx, int ny, int nz, double dx, double dy, double dz,
+                 int stride, GridDev* g, std::vector<Buf>* owned);
+
+CoefConst make_const(double a, double b, double az, double c, double d, double dz, double e, double dx, double dy,
+                     double dzs, int dim);
+
+inline dim3 stencil_block() { return dim3(kBx, kBy, 1); }
+dim3 stencil_grid(const GridDev& g, int zchunk = 16);
+dim3 stencil_grid_full(const GridDev& g, int zchunk = 16);
+inline int vec_blocks(long long n, const Context* ctx) {
+  long long b = (n + 255) / 256;
+  long long cap = (long long)ctx->num_sms * 8;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+// Dispatch on the coefficient form of a DevProblem: fn(coef) with the concrete type.
+template <class Fn>
+void with_coef(const DevProblem& P, Fn&& fn) {
+  switch (P.coef_kind) {
+    case kDivk: fn(P.cd); break;
+    case kNodal: fn(P.cn); break;
+    default: fn(P.cc); break;
+  }
+}
+
+void set_report_msg(pdeb200_report* r, const std::string& m);
+
+// Solver drivers (solvers.cu)
+pdeb200_status solve_dispatch(Context* ctx, DevProblem& P, const pdeb200_problem* hp, const pdeb200_options* o,
+                              double* d_out, pdeb200_report* rep);
+pdeb200_status residual_norms_dev(Context* ctx, DevProblem& P, const double* d_grid, double* l2, double* linf);
+pdeb200_status apply_dev(Context* ctx, DevProblem& P, const double* d_x, double* d_y);
+pdeb200_status time_series_dev(Context* ctx, DevProblem& P, const pdeb200_time_options* t, pdeb200_frame_cb cb,
+                               void* user, bool host_frames, double* d_out, pdeb200_report* rep);
+pdeb200_status project_dev(Context* ctx, int nx, int ny, int nz, double dx, double dy, double dz, double dt,
+                           double* u, double* v, double* w, double* p, const pdeb200_projection_options* po,
+                           pdeb200_projection_report* rep);
+
+}  // namespace pdeb

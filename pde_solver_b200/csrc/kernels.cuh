@@ -1,0 +1,521 @@
+// Kernels of libpdeb200. All stencil kernels use the same mapping: a thread
+// owns an (i,j) column and marches over a chunk of k, keeping the three
+// z-planes of the field it reads in registers (x/y neighbours come through
+// L1/L2). Blocks are 32 x 8 threads: a warp reads 32 consecutive doubles of
+// a row (fully coalesced 256 B).
+//
+// Every kernel of an iterative solve takes `ctl`, a device control block: when
+// ctl->done is set (convergence or breakdown found on the device) the kernel
+// returns at once. The host can therefore enqueue several iterations ahead and
+// poll lazily while the result stays exactly the one of stopping at the first
+// converged iteration.
+#pragma once
+
+#include "device.cuh"
+
+namespace pdeb {
+
+constexpr int kBx = 32;
+constexpr int kBy = 8;
+// capacity (in blocks) of the reduction partial buffers; launch shapes stay below it
+constexpr long long kMaxGridBlocks = 1LL << 17;
+
+struct Ctl {
+  int done;        // every kernel of the solve returns at once
+  int stop;        // relaxation: no further sweeps; closures still run
+  int status;      // pdeb200_status recorded with done/stop
+  int iter;        // completed iterations
+  int max_iter;
+  int pad;
+  double tol;      // absolute threshold (reference rules)
+  double tol2;     // squared threshold on the monitored norm (relative rule)
+  double brk;      // breakdown threshold on Krylov denominators
+  double rr;       // last monitored squared norm
+  double rz, pq, alpha, beta;             // CG family
+  double rho, rho_prev, omega, tt, ts;    // BiCGStab family
+  double bb;       // |b|^2
+  double delta;    // relaxation max |du|
+  double aux[8];
+};
+
+__device__ __forceinline__ bool ctl_skip(const Ctl* c) { return c && *((volatile const int*)&c->done); }
+__device__ __forceinline__ bool ctl_stopped(const Ctl* c) {
+  return c && (*((volatile const int*)&c->done) || *((volatile const int*)&c->stop));
+}
+
+__device__ __forceinline__ void column_range(const GridDev& g, int& k0, int& k1) {
+  // interior z range split into gridDim.z chunks
+  const int kb = g.dim == 3 ? 1 : 0;
+  const int ke = g.dim == 3 ? g.nz - 1 : 1;
+  const int len = ke - kb;
+  const int chunk = (len + gridDim.z - 1) / gridDim.z;
+  k0 = kb + blockIdx.z * chunk;
+  k1 = min(ke, k0 + chunk);
+}
+
+// ------------------------------------------------------------ folded apply
+
+// y = A_fold x on interior nodes (boundary rows of y untouched), with optional
+// fused sum(w * y) (w = x for p.Ap).
+template <class Coef, typename T, int NV, class Post>
+__global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, const T* __restrict__ x,
+                                                           T* __restrict__ y, RedSlot slot, Post post,
+                                                           const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  double acc[(NV > 0 ? NV : 1)] = {0.0};
+  const bool active = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
+  if (active && k0 < k1) {
+    long long id = ((long long)k0 * g.ny + j) * g.nx + i;
+    T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+    T zc = x[id];
+    for (int k = k0; k < k1; ++k, id += g.sxy) {
+      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+      Stencil<T> s = cf.template at<T>(g, id);
+      fold_faces<T>(g, i, j, k, s, nullptr);
+      const T v = s.c * zc + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim);
+      y[id] = v;
+      if constexpr (NV > 0) acc[0] += double(zc) * double(v);
+      zm = zc;
+      zc = zp;
+    }
+  }
+  if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
+}
+
+// r = b - A_fold x on interior nodes, optional fused |r|^2.
+template <class Coef, typename T, typename TB, int NV, class Post>
+__global__ void __launch_bounds__(kBx* kBy) k_residual_folded(GridDev g, Coef cf, const T* __restrict__ x,
+                                                              const TB* __restrict__ b, T* __restrict__ r,
+                                                              RedSlot slot, Post post, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  double acc[(NV > 0 ? NV : 1)] = {0.0};
+  const bool active = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
+  if (active && k0 < k1) {
+    long long id = ((long long)k0 * g.ny + j) * g.nx + i;
+    T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+    T zc = x[id];
+    for (int k = k0; k < k1; ++k, id += g.sxy) {
+      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+      Stencil<T> s = cf.template at<T>(g, id);
+      fold_faces<T>(g, i, j, k, s, nullptr);
+      const T v = T(b[id]) - (s.c * zc + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim));
+      r[id] = v;
+      if constexpr (NV > 0) acc[0] += double(v) * double(v);
+      zm = zc;
+      zc = zp;
+    }
+  }
+  if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
+}
+
+// Folded right-hand side b = -f - sum_faces w*c0 (boundary entries 0).
+template <class Coef>
+__global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, const double* __restrict__ f,
+                                                         double f_const, double* __restrict__ b) {
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2)) return;
+  for (int k = k0; k < k1; ++k) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    Stencil<double> s = cf.template at<double>(g, id);
+    double sh = 0.0;
+    fold_faces<double>(g, i, j, k, s, &sh);
+    b[id] = -(f ? f[id] : f_const) - sh;
+  }
+}
+
+// One red-black Gauss-Seidel colour pass on the folded operator; colour of
+// (i,j,k) is (i+j+k)&1. The updated colour only reads the other colour, so a
+// pass is race free.
+template <class Coef, typename T, typename TB>
+__global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x,
+                                                   int color, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) return;
+  int k = k0 + ((i + j + k0 + color) & 1);
+  for (; k < k1; k += 2) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    Stencil<T> s = cf.template at<T>(g, id);
+    fold_faces<T>(g, i, j, k, s, nullptr);
+    const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+    const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+    x[id] = (T(b[id]) - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
+  }
+}
+
+// ------------------------------------------------------------- full apply
+
+// y = L x with identity boundary rows: LinearOperator2D::Apply
+// (src/backends/cpu/cpu_utils.cpp:324-513) extended to 3D; optional fused
+// sum(w*y).
+template <class Coef, int NV, class Post>
+__global__ void __launch_bounds__(kBx* kBy) k_apply_full(GridDev g, Coef cf, const double* __restrict__ x,
+                                                         double* __restrict__ y, RedSlot slot, Post post,
+                                                         const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  // full z range (boundary planes included) split into chunks
+  const int chunk = (g.nz + gridDim.z - 1) / gridDim.z;
+  const int k0 = blockIdx.z * chunk, k1 = min(g.nz, k0 + chunk);
+  double acc[(NV > 0 ? NV : 1)] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    for (int k = k0; k < k1; ++k) {
+      const long long id = ((long long)k * g.ny + j) * g.nx + i;
+      const bool interior = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 &&
+                            (g.dim == 2 || (k >= 1 && k <= g.nz - 2));
+      double v;
+      if (interior) {
+        const Stencil<double> s = cf.template at<double>(g, id);
+        const double zp = g.dim == 3 ? x[id + g.sxy] : 0.0;
+        const double zm = g.dim == 3 ? x[id - g.sxy] : 0.0;
+        v = s.c * x[id] + nb_sum<double>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim);
+      } else {
+        v = x[id];
+      }
+      y[id] = v;
+      if constexpr (NV > 0) acc[0] += x[id] * v;
+    }
+  }
+  if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
+}
+
+// ---------------------------------------------------------------- Jacobi
+
+// One Jacobi sweep of the reference (relaxation.cpp:426-546, solver.cpp:808-962):
+// next = (-f - lap)/center on interior nodes, reading the stored face values of
+// `grid`; fused max|du| (the reference's stopping quantity).
+template <class Coef, class Post>
+__global__ void __launch_bounds__(kBx* kBy) k_jacobi(GridDev g, Coef cf, const double* __restrict__ f,
+                                                     double f_const, const double* __restrict__ grid,
+                                                     double* __restrict__ next, RedSlot slot, Post post,
+                                                     const Ctl* ctl, int* degenerate) {
+  if (ctl_stopped(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  double acc[1] = {0.0};
+  if (i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) {
+    for (int k = k0; k < k1; ++k) {
+      const long long id = ((long long)k * g.ny + j) * g.nx + i;
+      const Stencil<double> s = cf.template at<double>(g, id);
+      if (fabs(s.c) < 1e-12) {
+        *degenerate = 1;
+        continue;
+      }
+      const double zp = g.dim == 3 ? grid[id + g.sxy] : 0.0;
+      const double zm = g.dim == 3 ? grid[id - g.sxy] : 0.0;
+      const double lap = nb_sum<double>(s, grid[id + 1], grid[id - 1], grid[id + g.nx], grid[id - g.nx], zp, zm, g.dim);
+      const double rhs = -(f ? f[id] : f_const) - lap;
+      const double upd = __ddiv_rn(rhs, s.c);
+      next[id] = upd;
+      acc[0] = fmax(acc[0], fabs(upd - grid[id]));
+    }
+  }
+  grid_reduce<1, true>(acc, slot, post);
+}
+
+// -------------------------------------------------------- boundary fill
+
+// Final value of boundary node (i,j,k) after the reference's closure
+// sequence Dirichlet / Neumann-Robin (x faces, y faces, z faces) / Dirichlet
+// (src/backends/cpu/solver.cpp:751-753, cpu_utils.cpp:575-901):
+//  - a node on a Dirichlet face takes the value of the last Dirichlet face
+//    written (z over y over x, max over min);
+//  - otherwise the last Neumann/Robin phase containing it writes
+//    closure(u[inward neighbour]); the inward neighbour is either interior or a
+//    boundary node finalised by an earlier phase, so the chain is evaluated
+//    from the interior outwards (depth <= 3). Only interior nodes are read,
+//    so one launch over all faces is race free.
+__device__ __forceinline__ double closure_value(const FaceDev& f, int is_max, int loc, double unb,
+                                                bool* ok) {
+  *ok = true;
+  if (f.kind == kNeumann) {
+    const double gv = f.val.at(loc);
+    return is_max ? unb + f.h * gv : unb - f.h * gv;
+  }
+  const double alpha = f.alpha.at(loc), beta = f.beta.at(loc), gamma = f.gamma.at(loc);
+  if (!is_max) {
+    const double denom = alpha + beta / f.h;
+    if (fabs(denom) > 1e-12) return (gamma + (beta / f.h) * unb) / denom;
+  } else {
+    const double denom = alpha - beta / f.h;
+    if (fabs(denom) > 1e-12) return (gamma - (beta / f.h) * unb) / denom;
+  }
+  *ok = false;
+  return 0.0;
+}
+
+__device__ __forceinline__ int face_loc(const GridDev& g, int f, int i, int j, int k) {
+  return f <= kRight ? j + g.ny * k : (f <= kTop ? i + g.nx * k : i + g.nx * j);
+}
+
+__device__ __forceinline__ double boundary_final(const GridDev& g, const double* u, int i, int j, int k) {
+  // Dirichlet winner: back, front, top, bottom, right, left (reverse write order)
+  const bool on[6] = {i == 0, i == g.nx - 1, j == 0, j == g.ny - 1, g.dim == 3 && k == 0,
+                      g.dim == 3 && k == g.nz - 1};
+  for (int f = 5; f >= 0; --f)
+    if (on[f] && g.face[f].active && g.face[f].kind == kDirichlet) return g.face[f].val.at(face_loc(g, f, i, j, k));
+  int chain_f[3], chain_loc[3], cnt = 0;
+  int ci = i, cj = j, ck = k;
+  double base = 0.0;
+  for (int depth = 0; depth < 4; ++depth) {
+    const bool cb[6] = {ci == 0, ci == g.nx - 1, cj == 0, cj == g.ny - 1, g.dim == 3 && ck == 0,
+                        g.dim == 3 && ck == g.nz - 1};
+    int f = -1;
+    for (int q = 5; q >= 0; --q)
+      if (cb[q] && g.face[q].active) {
+        f = q;
+        break;
+      }
+    if (f < 0) {
+      base = u[((long long)ck * g.ny + cj) * g.nx + ci];
+      break;
+    }
+    if (g.face[f].kind == kDirichlet) {
+      base = g.face[f].val.at(face_loc(g, f, ci, cj, ck));
+      break;
+    }
+    chain_f[cnt] = f;
+    chain_loc[cnt] = face_loc(g, f, ci, cj, ck);
+    ++cnt;
+    if (f == kLeft) ci = 1;
+    else if (f == kRight) ci = g.nx - 2;
+    else if (f == kBottom) cj = 1;
+    else if (f == kTop) cj = g.ny - 2;
+    else if (f == kFront) ck = 1;
+    else ck = g.nz - 2;
+  }
+  double v = base;
+  for (int m = cnt - 1; m >= 0; --m) {
+    bool ok;
+    const double nv = closure_value(g.face[chain_f[m]], chain_f[m] & 1, chain_loc[m], v, &ok);
+    if (!ok) return u[((long long)k * g.ny + j) * g.nx + i];  // |denominator| <= 1e-12: node kept
+    v = nv;
+  }
+  return v;
+}
+
+// One thread per node of the six faces; a node shared by faces is written by
+// the first face (in face order) that contains it.
+static __global__ void k_fill_boundary(GridDev g, double* __restrict__ u, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const long long nxy = (long long)g.nx * g.ny;
+  const long long nyz = (long long)g.ny * g.nz, nxz = (long long)g.nx * g.nz;
+  const long long total = 2 * nyz + 2 * nxz + (g.dim == 3 ? 2 * nxy : 0);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k, f;
+    long long r = t;
+    if (r < 2 * nyz) {
+      f = r < nyz ? kLeft : kRight;
+      r %= nyz;
+      j = int(r % g.ny);
+      k = int(r / g.ny);
+      i = f == kLeft ? 0 : g.nx - 1;
+    } else if ((r -= 2 * nyz) < 2 * nxz) {
+      f = r < nxz ? kBottom : kTop;
+      r %= nxz;
+      i = int(r % g.nx);
+      k = int(r / g.nx);
+      j = f == kBottom ? 0 : g.ny - 1;
+    } else {
+      r -= 2 * nxz;
+      f = r < nxy ? kFront : kBack;
+      r %= nxy;
+      i = int(r % g.nx);
+      j = int(r / g.nx);
+      k = f == kFront ? 0 : g.nz - 1;
+    }
+    // ownership: the first face in face order containing the node
+    const bool on[6] = {i == 0, i == g.nx - 1, j == 0, j == g.ny - 1, g.dim == 3 && k == 0,
+                        g.dim == 3 && k == g.nz - 1};
+    int owner = -1;
+    for (int q = 0; q < 6; ++q)
+      if (on[q]) {
+        owner = q;
+        break;
+      }
+    if (owner != f) continue;
+    u[((long long)k * g.ny + j) * g.nx + i] = boundary_final(g, u, i, j, k);
+  }
+}
+
+// ------------------------------------------------------------ 1D vectors
+
+__device__ __forceinline__ long long gtid() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ long long gstride() { return (long long)gridDim.x * blockDim.x; }
+
+// x += alpha p ; r -= alpha q ; |r|^2   (alpha = ctl->alpha)
+template <typename T, class Post>
+__global__ void k_cg_xr(long long n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                        const T* __restrict__ q, RedSlot slot, Post post, Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const double a = ctl->alpha;
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < n; t += gstride()) {
+    x[t] = T(double(x[t]) + a * double(p[t]));
+    const T rv = T(double(r[t]) - a * double(q[t]));
+    r[t] = rv;
+    acc[0] += double(rv) * double(rv);
+  }
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+// p = z + beta p (beta = ctl->beta; first iteration: p = z)
+template <typename T>
+__global__ void k_cg_p(long long n, T* __restrict__ p, const T* __restrict__ z, const Ctl* ctl, int first) {
+  if (ctl_skip(ctl)) return;
+  const double bta = first ? 0.0 : ctl->beta;
+  for (long long t = gtid(); t < n; t += gstride()) p[t] = first ? z[t] : T(double(z[t]) + bta * double(p[t]));
+}
+
+// sum(a*b) with post
+template <typename T, class Post>
+__global__ void k_dot(long long n, const T* __restrict__ a, const T* __restrict__ b, RedSlot slot, Post post,
+                      const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < n; t += gstride()) acc[0] += double(a[t]) * double(b[t]);
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+// two dots at once: sum(a*b), sum(c*d)
+template <typename T, class Post>
+__global__ void k_dot2(long long n, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ c,
+                       const T* __restrict__ d, RedSlot slot, Post post, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  double acc[2] = {0.0, 0.0};
+  for (long long t = gtid(); t < n; t += gstride()) {
+    acc[0] += double(a[t]) * double(b[t]);
+    acc[1] += double(c[t]) * double(d[t]);
+  }
+  grid_reduce<2, false>(acc, slot, post);
+}
+
+template <typename TD, typename TS>
+__global__ void k_convert(long long n, TD* __restrict__ dst, const TS* __restrict__ src) {
+  for (long long t = gtid(); t < n; t += gstride()) dst[t] = TD(src[t]);
+}
+
+template <typename T>
+__global__ void k_fill(long long n, T* __restrict__ dst, T v, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  for (long long t = gtid(); t < n; t += gstride()) dst[t] = v;
+}
+
+// ------------------------------------------------------------ multigrid
+
+// Full weighting (tensor [1/4,1/2,1/4]) of the fine residual onto interior
+// coarse nodes, n_c = (n_f+1)/2 (multigrid.cpp:14-36 in 2D, trilinear in 3D).
+template <typename T, typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_restrict(GridDev gf, GridDev gc, const T* __restrict__ rf,
+                                                       TC* __restrict__ bc, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int I = blockIdx.x * kBx + threadIdx.x;
+  const int J = blockIdx.y * kBy + threadIdx.y;
+  int K0, K1;
+  column_range(gc, K0, K1);
+  if (!(I >= 1 && I <= gc.nx - 2 && J >= 1 && J <= gc.ny - 2)) return;
+  const double w[3] = {0.25, 0.5, 0.25};
+  for (int K = K0; K < K1; ++K) {
+    double acc = 0.0;
+    const int kf = gc.dim == 3 ? 2 * K : 0;
+    const long long base = ((long long)kf * gf.ny + 2 * J) * gf.nx + 2 * I;
+    if (gc.dim == 3) {
+#pragma unroll
+      for (int dk = -1; dk <= 1; ++dk)
+#pragma unroll
+        for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+          for (int di = -1; di <= 1; ++di)
+            acc += w[di + 1] * w[dj + 1] * w[dk + 1] * double(rf[base + dk * gf.sxy + dj * gf.nx + di]);
+    } else {
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) acc += w[di + 1] * w[dj + 1] * double(rf[base + dj * gf.nx + di]);
+    }
+    bc[((long long)K * gc.ny + J) * gc.nx + I] = TC(acc);
+  }
+}
+
+// Trilinear (bilinear in 2D) prolongation of the coarse correction added to
+// the fine interior (multigrid.cpp:38-67); the coarse boundary is zero.
+template <typename T, typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc, const TC* __restrict__ xc,
+                                                          T* __restrict__ xf, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(gf, k0, k1);
+  if (!(i >= 1 && i <= gf.nx - 2 && j >= 1 && j <= gf.ny - 2)) return;
+  const int I0 = i >> 1, I1 = (i + 1) >> 1, J0 = j >> 1, J1 = (j + 1) >> 1;
+  for (int k = k0; k < k1; ++k) {
+    const int K0 = gf.dim == 3 ? k >> 1 : 0, K1 = gf.dim == 3 ? (k + 1) >> 1 : 0;
+    const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
+    const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
+    const double v = 0.125 * (double(xc[a0 + r0 + I0]) + double(xc[a0 + r0 + I1]) + double(xc[a0 + r1 + I0]) +
+                              double(xc[a0 + r1 + I1]) + double(xc[a1 + r0 + I0]) + double(xc[a1 + r0 + I1]) +
+                              double(xc[a1 + r1 + I0]) + double(xc[a1 + r1 + I1]));
+    const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
+    xf[id] = T(double(xf[id]) + v);
+  }
+}
+
+// Coarse k by injection k_c(I,J,K) = k_f(2I,2J,2K).
+template <typename KT>
+__global__ void k_inject(GridDev gf, GridDev gc, const KT* __restrict__ kf, KT* __restrict__ kc) {
+  for (long long t = gtid(); t < gc.n; t += gstride()) {
+    const int I = int(t % gc.nx);
+    const int J = int((t / gc.nx) % gc.ny);
+    const int K = int(t / gc.sxy);
+    kc[t] = kf[((long long)(gc.dim == 3 ? 2 * K : 0) * gf.ny + 2 * J) * gf.nx + 2 * I];
+  }
+}
+
+// Coarsest level: `sweeps` red-black GS sweeps from zero, one block.
+template <class Coef, typename T, typename TB>
+__global__ void k_coarse_solve(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x, int sweeps,
+                               const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int tid = threadIdx.x;
+  for (long long t = tid; t < g.n; t += blockDim.x) x[t] = T(0);
+  __syncthreads();
+  const int kb = g.dim == 3 ? 1 : 0, ke = g.dim == 3 ? g.nz - 1 : 1;
+  const int ni = g.nx - 2, nj = g.ny - 2, nk = ke - kb;
+  const int total = ni * nj * nk;
+  for (int s = 0; s < sweeps; ++s) {
+    for (int color = 0; color < 2; ++color) {
+      for (int t = tid; t < total; t += blockDim.x) {
+        const int i = 1 + t % ni, j = 1 + (t / ni) % nj, k = kb + t / (ni * nj);
+        if (((i + j + k) & 1) != color) continue;
+        const long long id = ((long long)k * g.ny + j) * g.nx + i;
+        Stencil<T> st = cf.template at<T>(g, id);
+        fold_faces<T>(g, i, j, k, st, nullptr);
+        const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+        const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+        x[id] = (T(b[id]) - nb_sum<T>(st, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / st.c;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace pdeb

@@ -1,0 +1,450 @@
+// Templates shared by the solver drivers: device-side post functors of the
+// fused reductions, the enqueue/poll driver, the geometric MG hierarchy with
+// its V-cycle, right-hand-side builders and residual reports.
+#pragma once
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "host.h"
+
+namespace pdeb {
+
+// ------------------------------------------------------------------ posts
+
+struct PostBBOnly {
+  Ctl* c;
+  __device__ void operator()(const double* v) const { c->bb = v[0]; }
+};
+
+struct PostStoreRR {
+  Ctl* c;
+  __device__ void operator()(const double* v) const { c->rr = v[0]; }
+};
+
+// alpha = rz / pq  (breakdown when |pq| < brk or not finite)
+struct PostAlpha {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->pq = v[0];
+    if (!(fabs(v[0]) >= c->brk) || isnan(v[0])) {
+      c->done = 1;
+      c->status = PDEB200_ERR_BREAKDOWN;
+      return;
+    }
+    c->alpha = c->rz / v[0];
+  }
+};
+
+// relative rule on |r|^2 <= tol2
+struct PostRRRel {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->rr = v[0];
+    c->iter += 1;
+    if (v[0] <= c->tol2) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+    } else if (isnan(v[0])) {
+      c->done = 1;
+      c->status = PDEB200_ERR_BREAKDOWN;
+    } else if (c->iter >= c->max_iter) {
+      c->done = 1;
+      c->status = PDEB200_ERR_NOT_CONVERGED;
+    }
+  }
+};
+
+// reference CG (krylov.cpp:58-77): stop when sqrt(rr_new) < tol, else
+// beta = rr_new/rr and rr = rr_new
+struct PostRRRefCG {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->rr = v[0];
+    c->iter += 1;
+    if (sqrt(v[0]) < c->tol) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+    } else if (c->iter >= c->max_iter) {
+      c->done = 1;
+      c->status = PDEB200_ERR_NOT_CONVERGED;
+    } else {
+      c->beta = v[0] / c->rz;
+      c->rz = v[0];
+    }
+  }
+};
+
+struct PostBeta {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->beta = v[0] / c->rz;
+    c->rz = v[0];
+  }
+};
+
+struct PostRZ {
+  Ctl* c;
+  __device__ void operator()(const double* v) const { c->rz = v[0]; }
+};
+
+// |b|^2 of the relative rule: tol2 = tol^2 |b|^2, immediate exit for b = 0
+struct PostBB {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->bb = v[0];
+    c->rr = v[0];
+    c->tol2 = c->tol * c->tol * v[0];
+    if (v[0] == 0.0) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+    }
+  }
+};
+
+// initial |r|^2 of the reference CG: exit when sqrt(rr) < tol before iterating
+struct PostRR0Ref {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->rr = v[0];
+    c->rz = v[0];
+    if (sqrt(v[0]) < c->tol) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+    }
+  }
+};
+
+// relaxation: max|du| < tol stops sweeping (relaxation.cpp:557, solver.cpp:976)
+struct PostDelta {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->delta = v[0];
+    c->iter += 1;
+    if (v[0] < c->tol) {
+      c->stop = 1;
+      c->status = PDEB200_OK;
+    } else if (c->iter >= c->max_iter) {
+      c->stop = 1;
+      c->status = PDEB200_ERR_NOT_CONVERGED;
+    }
+  }
+};
+
+// ------------------------------------------------------------- utilities
+
+inline void ctl_init(Context* ctx, int max_iter, double tol, double brk) {
+  std::memset(ctx->h_ctl, 0, sizeof(Ctl));
+  ctx->h_ctl->max_iter = max_iter;
+  ctx->h_ctl->tol = tol;
+  ctx->h_ctl->brk = brk;
+  ctx->h_ctl->status = PDEB200_ERR_NOT_CONVERGED;
+  PDEB_CUDA(cudaMemcpyAsync(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+inline const Ctl& ctl_poll(Context* ctx) {
+  PDEB_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return *ctx->h_ctl;
+}
+
+inline void ctl_set_done(Context* ctx, int status) {
+  int v[3] = {1, 1, status};
+  PDEB_CUDA(cudaMemcpyAsync(ctx->d_ctl, v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// Enqueue iterations in growing batches and poll; `iterate()` enqueues one
+// iteration. Returns when the device reports done/stop or the cancel flag is set.
+template <class It>
+pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& iterate, bool use_stop) {
+  int enq = 0;
+  int batch = 1;
+  const int cap = o->check_interval > 0 ? o->check_interval : 16;
+  while (true) {
+    for (int b = 0; b < batch && enq < max_iter; ++b, ++enq) iterate(enq);
+    const Ctl& c = ctl_poll(ctx);
+    if (c.done || (use_stop && c.stop)) return (pdeb200_status)c.status;
+    if (enq >= max_iter) return PDEB200_ERR_NOT_CONVERGED;
+    if (o->cancel && *o->cancel) {
+      ctl_set_done(ctx, PDEB200_ERR_CANCELLED);
+      return PDEB200_ERR_CANCELLED;
+    }
+    batch = batch * 2 < cap ? batch * 2 : cap;
+  }
+}
+
+inline void fill_boundary(Context* ctx, const GridDev& g, double* u, const Ctl* ctl) {
+  const long long faces = 2LL * g.ny * g.nz + 2LL * g.nx * g.nz + (g.dim == 3 ? 2LL * g.nx * g.ny : 0);
+  const int blocks = vec_blocks(faces, ctx);
+  k_fill_boundary<<<blocks, 256, 0, ctx->stream>>>(g, u, ctl);
+  ctx->count();
+}
+
+template <typename T>
+void vfill(Context* ctx, long long n, T* p, T v, const Ctl* ctl) {
+  k_fill<T><<<vec_blocks(n, ctx), 256, 0, ctx->stream>>>(n, p, v, ctl);
+  ctx->count();
+}
+
+
+// ------------------------------------------------------------ rhs builders
+
+// BuildRhs2D (src/backends/cpu/solver.cpp:167-232), any dimension: Dirichlet
+// values on boundary nodes (last Dirichlet face written wins, 0 elsewhere),
+// -f in the interior.
+__global__ void k_full_rhs(GridDev g, const double* __restrict__ f, double f_const, double* __restrict__ b);
+
+inline void build_full_rhs(Context* ctx, DevProblem& P, double* b) {
+  k_full_rhs<<<vec_blocks(P.g.n, ctx), 256, 0, ctx->stream>>>(P.g, P.f, P.f_const, b);
+  ctx->count();
+}
+
+template <class Coef>
+void build_folded_rhs(Context* ctx, DevProblem& P, const Coef& cf, double* b) {
+  PDEB_CUDA(cudaMemsetAsync(b, 0, sizeof(double) * P.g.n, ctx->stream));
+  k_folded_rhs<Coef><<<stencil_grid(P.g), stencil_block(), 0, ctx->stream>>>(P.g, cf, P.f, P.f_const, b);
+  ctx->count();
+}
+
+// sum over all nodes of (b - L x)^2 with identity boundary rows
+template <class Coef, class Post>
+__global__ void __launch_bounds__(kBx* kBy) k_residual_full(GridDev g, Coef cf, const double* __restrict__ x,
+                                                            const double* __restrict__ b, RedSlot slot, Post post) {
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  const int chunk = (g.nz + gridDim.z - 1) / gridDim.z;
+  const int k0 = blockIdx.z * chunk, k1 = min(g.nz, k0 + chunk);
+  double acc[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    for (int k = k0; k < k1; ++k) {
+      const long long id = ((long long)k * g.ny + j) * g.nx + i;
+      const bool interior = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 &&
+                            (g.dim == 2 || (k >= 1 && k <= g.nz - 2));
+      double v = x[id];
+      if (interior) {
+        const Stencil<double> s = cf.template at<double>(g, id);
+        const double zp = g.dim == 3 ? x[id + g.sxy] : 0.0;
+        const double zm = g.dim == 3 ? x[id - g.sxy] : 0.0;
+        v = s.c * x[id] + nb_sum<double>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim);
+      }
+      const double r = b[id] - v;
+      acc[0] += r * r;
+    }
+  }
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+template <class Coef>
+void full_residual_report(Context* ctx, DevProblem& P, const Coef& cf, const double* b, const double* x, double*,
+                          pdeb200_report* rep) {
+  if (!rep) return;
+  const long long n = P.g.n;
+  k_residual_full<Coef, PostStoreRR><<<stencil_grid_full(P.g), stencil_block(), 0, ctx->stream>>>(
+      P.g, cf, x, b, ctx->slot(), PostStoreRR{ctx->d_ctl});
+  k_dot<double, PostBBOnly><<<vec_blocks(n, ctx), 256, 0, ctx->stream>>>(n, b, b, ctx->slot(1),
+                                                                       PostBBOnly{ctx->d_ctl}, nullptr);
+  ctx->count(2);
+  const Ctl& c = ctl_poll(ctx);
+  rep->residual_l2 = std::sqrt(c.rr);
+  rep->rhs_l2 = std::sqrt(c.bb);
+  rep->rel_residual = c.bb > 0 ? rep->residual_l2 / rep->rhs_l2 : 0.0;
+}
+
+template <class Coef>
+void folded_residual_report(Context* ctx, DevProblem& P, const Coef& cf, const double* bf, const double* x,
+                            double* scratch, pdeb200_report* rep) {
+  if (!rep) return;
+  const long long n = P.g.n;
+  k_residual_folded<Coef, double, double, 1, PostStoreRR><<<stencil_grid(P.g), stencil_block(), 0, ctx->stream>>>(
+      P.g, cf, x, bf, scratch, ctx->slot(), PostStoreRR{ctx->d_ctl}, nullptr);
+  k_dot<double, PostBBOnly><<<vec_blocks(n, ctx), 256, 0, ctx->stream>>>(n, bf, bf, ctx->slot(1),
+                                                                        PostBBOnly{ctx->d_ctl}, nullptr);
+  ctx->count(2);
+  const Ctl& c = ctl_poll(ctx);
+  rep->residual_l2 = std::sqrt(c.rr);
+  rep->rhs_l2 = std::sqrt(c.bb);
+  rep->rel_residual = c.bb > 0 ? rep->residual_l2 / rep->rhs_l2 : 0.0;
+}
+
+// ------------------------------------------------------------ MG hierarchy
+
+inline bool can_coarsen(const GridDev& g) {
+  if (!(g.nx >= 5 && (g.nx & 1) && g.ny >= 5 && (g.ny & 1))) return false;
+  if (g.dim == 3 && !(g.nz >= 5 && (g.nz & 1))) return false;
+  return true;
+}
+
+template <typename KT>
+inline void inject_k(Context* ctx, const GridDev& gf, const GridDev& gc, const KT* kf, KT* kc) {
+  k_inject<KT><<<vec_blocks(gc.n, ctx), 256, 0, ctx->stream>>>(gf, gc, kf, kc);
+  ctx->count();
+}
+
+// Coarse coefficients: constants are re-evaluated with the coarse spacing,
+// sampled fields are injected (k_c(I) = k_f(2I)).
+inline CoefConst coarsen_coef(Context*, const DevProblem& P, const CoefConst&, const GridDev&, const GridDev& gc,
+                              double dx, double dy, double dz, std::vector<Buf>*) {
+  return make_const(P.a, P.b, P.az, P.c, P.d, P.dzc, P.e, dx, dy, dz, gc.dim);
+}
+
+template <typename KT>
+inline CoefDivk<KT> coarsen_coef(Context* ctx, const DevProblem& P, const CoefDivk<KT>& f, const GridDev& gf,
+                                 const GridDev& gc, double dx, double dy, double dz, std::vector<Buf>* owned) {
+  CoefDivk<KT> c = f;
+  owned->emplace_back(sizeof(KT) * gc.n, ctx->stream);
+  KT* kc = owned->back().template as<KT>();
+  inject_k<KT>(ctx, gf, gc, f.k, kc);
+  c.k = kc;
+  c.ihx2 = 1.0 / (dx * dx);
+  c.ihy2 = 1.0 / (dy * dy);
+  c.ihz2 = gc.dim == 3 ? 1.0 / (dz * dz) : 0.0;
+  c.cx = P.c / (2.0 * dx);
+  c.dyc = P.d / (2.0 * dy);
+  c.dzc = gc.dim == 3 ? P.dzc / (2.0 * dz) : 0.0;
+  return c;
+}
+
+inline CoefNodal coarsen_coef(Context* ctx, const DevProblem&, const CoefNodal& f, const GridDev& gf,
+                              const GridDev& gc, double dx, double dy, double dz, std::vector<Buf>* owned) {
+  CoefNodal c = f;
+  owned->emplace_back(sizeof(double) * 7 * gc.n, ctx->stream);
+  double* dst = owned->back().as<double>();
+  for (int q = 0; q < 7; ++q) inject_k<double>(ctx, gf, gc, f.nodal + (long long)q * f.n, dst + (long long)q * gc.n);
+  c.nodal = dst;
+  c.n = gc.n;
+  c.dx2 = dx * dx;
+  c.dy2 = dy * dy;
+  c.dz2 = dz * dz;
+  c.tdx = 2.0 * dx;
+  c.tdy = 2.0 * dy;
+  c.tdz = 2.0 * dz;
+  return c;
+}
+
+// Geometric hierarchy of the folded operator. Coarsening n_c = (n+1)/2 while
+// every active dimension is odd and >= 5, stopping once a dimension reaches 5
+// or mg_max_levels (the rule of multigrid.cpp:150-170); face closures are
+// rediscretised with the coarse spacing. Vectors of type T.
+template <class Coef, typename T>
+struct Hierarchy {
+  struct Level {
+    GridDev g;
+    Coef cf;
+    T* x;
+    T* b;
+    T* r;
+  };
+  std::vector<Level> levels;
+  std::vector<Buf> owned;
+  int pre = 2, post = 2, coarse_iters = 50;
+
+  T* alloc(Context* ctx, long long n) {
+    owned.emplace_back(sizeof(T) * n, ctx->stream);
+    T* p = owned.back().template as<T>();
+    PDEB_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * n, ctx->stream));
+    return p;
+  }
+
+  void build(Context* ctx, DevProblem& P, const pdeb200_problem* hp, const Coef& cf0, const pdeb200_options* o) {
+    pre = o->mg_pre_smooth > 0 ? o->mg_pre_smooth : 0;
+    post = o->mg_post_smooth > 0 ? o->mg_post_smooth : 0;
+    coarse_iters = o->mg_coarse_iters > 1 ? o->mg_coarse_iters : 1;
+    const int max_levels = o->mg_max_levels > 1 ? o->mg_max_levels : 1;
+    Level l0;
+    l0.g = P.g;
+    l0.cf = cf0;
+    l0.x = alloc(ctx, P.g.n);
+    l0.b = nullptr;
+    l0.r = alloc(ctx, P.g.n);
+    levels.push_back(l0);
+    double dx = P.dx, dy = P.dy, dz = P.dz;
+    int stride = 1;
+    while ((int)levels.size() < max_levels && can_coarsen(levels.back().g)) {
+      const GridDev& gf = levels.back().g;
+      Level c;
+      c.g = gf;
+      c.g.nx = (gf.nx + 1) / 2;
+      c.g.ny = (gf.ny + 1) / 2;
+      c.g.nz = gf.dim == 3 ? (gf.nz + 1) / 2 : 1;
+      c.g.sxy = (long long)c.g.nx * c.g.ny;
+      c.g.n = c.g.sxy * c.g.nz;
+      dx *= 2.0;
+      dy *= 2.0;
+      if (gf.dim == 3) dz *= 2.0;
+      stride *= 2;
+      // exact coarse spacing from the domain, as the reference recomputes it
+      const double cdx = (hp->xmax - hp->xmin) / (double)(c.g.nx - 1);
+      const double cdy = (hp->ymax - hp->ymin) / (double)(c.g.ny - 1);
+      const double cdz = gf.dim == 3 ? (hp->zmax - hp->zmin) / (double)(c.g.nz - 1) : 0.0;
+      build_faces(ctx, hp, c.g.nx, c.g.ny, c.g.nz, cdx, cdy, cdz, stride, &c.g, &owned);
+      c.cf = coarsen_coef(ctx, P, levels.back().cf, gf, c.g, cdx, cdy, cdz, &owned);
+      c.x = alloc(ctx, c.g.n);
+      c.b = alloc(ctx, c.g.n);
+      c.r = alloc(ctx, c.g.n);
+      levels.push_back(c);
+      if (c.g.nx <= 5 || c.g.ny <= 5 || (c.g.dim == 3 && c.g.nz <= 5)) break;
+    }
+  }
+
+  void smooth(Context* ctx, const Level& L, const T* b, int sweeps, bool reverse, const Ctl* ctl) {
+    const dim3 grid = stencil_grid(L.g), block = stencil_block();
+    for (int s = 0; s < sweeps; ++s) {
+      k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, reverse ? 1 : 0, ctl);
+      k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, reverse ? 0 : 1, ctl);
+      ctx->count(2);
+    }
+  }
+
+  void level(Context* ctx, int l, const T* rhs0, const Ctl* ctl) {
+    Level& L = levels[l];
+    const T* b = l == 0 ? rhs0 : L.b;
+    vfill<T>(ctx, L.g.n, L.x, T(0), ctl);
+    if (l == (int)levels.size() - 1) {
+      if (L.g.n <= 65536) {
+        k_coarse_solve<Coef, T, T><<<1, 256, 0, ctx->stream>>>(L.g, L.cf, b, L.x, coarse_iters, ctl);
+        ctx->count();
+      } else {
+        smooth(ctx, L, b, coarse_iters, false, ctl);
+      }
+      return;
+    }
+    smooth(ctx, L, b, pre, false, ctl);
+    k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(
+        L.g, L.cf, L.x, b, L.r, RedSlot{}, NoPost{}, ctl);
+    Level& C = levels[l + 1];
+    k_restrict<T, T><<<stencil_grid(C.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+    ctx->count(2);
+    level(ctx, l + 1, rhs0, ctl);
+    k_prolong_add<T, T><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.x, L.x, ctl);
+    ctx->count();
+    smooth(ctx, L, b, post, true, ctl);
+  }
+
+  // z = M rhs0, result in levels[0].x
+  void vcycle(Context* ctx, const T* rhs0, const Ctl* ctl) { level(ctx, 0, rhs0, ctl); }
+};
+
+// -------------------------------------------------- drivers in other units
+
+template <class Coef>
+pdeb200_status gauss_seidel(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o, double* d_out,
+                            pdeb200_report* rep);
+template <class Coef>
+pdeb200_status bicgstab_reference(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o,
+                                  double* d_x, pdeb200_report* rep);
+template <class Coef>
+pdeb200_status gmres_reference(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o, double* d_x,
+                               pdeb200_report* rep);
+pdeb200_status mg_vcycle_reference(Context* ctx, DevProblem& P, const pdeb200_problem* hp, const pdeb200_options* o,
+                                   double* d_out, pdeb200_report* rep);
+template <class Coef>
+pdeb200_status mixed_refinement(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_problem* hp,
+                                const pdeb200_options* o, double* d_x, pdeb200_report* rep);
+template <class Coef>
+pdeb200_status mg_bicgstab(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_problem* hp,
+                           const pdeb200_options* o, double* d_x, pdeb200_report* rep);
+
+}  // namespace pdeb

@@ -1,0 +1,112 @@
+"""Python host API over the C ABI (include/pdeb200.h).
+
+Mirrors the reference's solve entry (SolveWithBackend / SolvePDECuda,
+src/backend_solve.cpp:53, src/backends/cuda/CudaSolve.cu:31): a problem and
+solver options in, the full grid field out, errors as a status and message.
+Every call goes through libpdeb200.so; there is no other implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .problem import GridProblem, default_options
+
+
+class SolveError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+        self.message = message
+
+
+def _lib():
+    return abi.load()
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def solve(problem: GridProblem, options: abi.Options | None = None, out=None, raise_on_error=True, **kw):
+    """Steady solve. Returns (field, report). With MEM_DEVICE problems `out`
+    must be a device pointer (int) and is returned as given."""
+    lib = _lib()
+    opt = options if options is not None else default_options(**kw)
+    rep = abi.Report()
+    cp = problem.to_c()
+    if problem.mem_space == abi.MEM_DEVICE:
+        assert out is not None, "device problems need a device output pointer"
+        st = lib.pdeb200_solve(C.byref(cp), C.byref(opt), C.c_void_p(out), C.byref(rep))
+        res = out
+    else:
+        res = np.empty(problem.n) if out is None else out
+        st = lib.pdeb200_solve(C.byref(cp), C.byref(opt), res.ctypes.data_as(C.c_void_p), C.byref(rep))
+    if st != abi.OK and raise_on_error and st != abi.ERR_NOT_CONVERGED:
+        raise SolveError(st, rep.message.decode() or lib.pdeb200_status_string(st).decode())
+    rep.status = st
+    return res, rep
+
+
+def apply(problem: GridProblem, x, device: int = 0):
+    lib = _lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    cp = problem.to_c()
+    st = lib.pdeb200_apply(C.byref(cp), x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), device)
+    if st != abi.OK:
+        raise SolveError(st, lib.pdeb200_status_string(st).decode())
+    return y
+
+
+def residual_norms(problem: GridProblem, grid, device: int = 0):
+    lib = _lib()
+    grid = np.ascontiguousarray(grid, dtype=np.float64)
+    l2, linf = C.c_double(), C.c_double()
+    cp = problem.to_c()
+    st = lib.pdeb200_residual_norms(C.byref(cp), grid.ctypes.data_as(C.c_void_p), device, C.byref(l2), C.byref(linf))
+    if st != abi.OK:
+        raise SolveError(st, lib.pdeb200_status_string(st).decode())
+    return l2.value, linf.value
+
+
+def time_series(problem: GridProblem, t_start: float, dt: float, frames: int, on_frame=None, device: int = 0,
+                frame_stride: int = 1):
+    """Forward-Euler frames (SolvePDETimeSeries). on_frame(frame, t, grid) -> bool."""
+    lib = _lib()
+    to = abi.TimeOptions(t_start=t_start, dt=dt, frames=frames, frame_stride=frame_stride, device=device)
+    out = np.empty(problem.n)
+    n = problem.n
+
+    def _cb(frame, t, ptr, user):
+        if on_frame is None:
+            return 1
+        arr = np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+        return 1 if on_frame(frame, t, arr) is not False else 0
+
+    cb = abi.FRAME_CB(_cb)
+    rep = abi.Report()
+    cp = problem.to_c()
+    st = lib.pdeb200_time_series(C.byref(cp), C.byref(to), cb, None, out.ctypes.data_as(C.c_void_p), C.byref(rep))
+    if st != abi.OK:
+        raise SolveError(st, rep.message.decode() or lib.pdeb200_status_string(st).decode())
+    return out, rep
+
+
+def project_velocity(u, v, w, p, nx, ny, nz, dx, dy, dz, dt, max_iter=1000, tol=1e-8, fix_corner=True,
+                     device=0):
+    """ProjectVelocity2D/3D; arrays are updated copies (u, v, w, p, report)."""
+    lib = _lib()
+    u, v, p = (np.array(a, dtype=np.float64) for a in (u, v, p))
+    w = np.array(w, dtype=np.float64) if w is not None else None
+    po = abi.ProjectionOptions(max_iter=max_iter, fix_pressure_corner=int(fix_corner), tol=tol, device=device,
+                               mem_space=abi.MEM_HOST)
+    rep = abi.ProjectionReport()
+    st = lib.pdeb200_project_velocity(nx, ny, nz, dx, dy, dz, dt, u.ctypes.data_as(C.c_void_p),
+                                      v.ctypes.data_as(C.c_void_p),
+                                      w.ctypes.data_as(C.c_void_p) if w is not None else None,
+                                      p.ctypes.data_as(C.c_void_p), C.byref(po), C.byref(rep))
+    rep.status = st
+    return u, v, w, p, rep
