@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Headline benchmark: solves/s of the 3D variable-coefficient Poisson solve
+-div(k grad u) = F on [0,1]^3 with 257^3 nodes, k log-normal (sigma=1) smoothed
+by 3 box passes, F ~ N(0,1), mixed Dirichlet/Neumann/Robin(1,1,0) faces,
+geometric-MG V(2,2)-preconditioned CG with red-black Gauss-Seidel, FP64, to
+1e-10 relative residual (the reference's CPU path cannot express this
+divergence-form problem; the CPU baseline is the oracle port of the same
+algorithm).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+A step is one complete solve. `value` is measured with k and f resident in
+HBM (device pointers); `e2e` goes through the same C-ABI call with pinned host
+buffers, so every step includes the H2D copy of k and f and the D2H copy of the
+solution. Multi-GPU runs are independent replicas (no collective on the data
+path); each rank solves its own copy and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "solves/s (3D var-k Poisson 257^3, MG-PCG FP64 to 1e-10 rel. residual)"
+UNIT = "solves/s"
+N_DEFAULT = 257
+SEED = 1234
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(n, l2_note):
+    return {"workload": f"3D variable-k Poisson {n}^3, MG V(2,2)-PCG red-black GS, FP64, rel. residual 1e-10",
+            "grid": [n, n, n], "dofs": n ** 3, "k": "log-normal sigma=1, 3 box passes", "f": "N(0,1)",
+            "faces": "left/right D0, bottom/top N0, front Robin(1,1,0), back D0", "seed": SEED,
+            "parallelism": "replicas", "l2": l2_note}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_name):
+    """DRAM bytes per launch of `kernel_name` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel_name:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower().startswith("active")})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU side
+
+def cpu_sample(prob, gpu_iters):
+    """Oracle port of the same MG-PCG on the host cores (OpenMP, all threads):
+    setup + 1 iteration and setup + 3 iterations on the same 257^3 input give
+    the per-iteration cost; a solve is setup + iterations-to-converge."""
+    from oracle import oracle
+    from pde_solver_b200 import abi
+    from pde_solver_b200.problem import default_options
+
+    cores = os.cpu_count() or 1
+    oracle.build(ref=False)
+    oracle.restate().rs_set_threads(cores)
+    times = {}
+    for its in (1, 3):
+        o = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=its)
+        t0 = time.perf_counter()
+        oracle.rs_solve(prob, o)
+        times[its] = time.perf_counter() - t0
+    t_iter = max((times[3] - times[1]) / 2.0, 1e-9)
+    t_setup = max(times[1] - t_iter, 0.0)
+    t_solve = t_setup + gpu_iters * t_iter
+    return {"value": 1.0 / t_solve, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"oracle/restate.c MG-PCG on the same {prob.nx}^3 input, OpenMP {cores} threads: "
+                       f"setup+1 and setup+3 iterations timed ({times[1]:.2f}s, {times[3]:.2f}s), "
+                       f"solve = setup + {gpu_iters} iterations = {t_solve:.2f}s")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    from pde_solver_b200 import abi, synthetic
+    from pde_solver_b200.problem import default_options
+
+    cores = os.cpu_count() or 1
+    oracle.build(ref=False)
+    oracle.restate().rs_set_threads(cores)
+    prob = synthetic.varcoef_poisson_3d(args.n, seed=SEED)
+    full = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400)
+    # warm-up: one converged solve fixes the iteration count of this input
+    t0 = time.perf_counter()
+    st, _, rep = oracle.rs_solve(prob, full)
+    t_full = time.perf_counter() - t0
+    iters = rep.iterations
+    one = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=1)
+    three = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=3)
+    for _ in range(max(args.warmup - 1, 0)):
+        oracle.rs_solve(prob, one)
+    t3 = []
+    t0 = time.perf_counter()
+    oracle.rs_solve(prob, three)
+    t3.append(time.perf_counter() - t0)
+    samples = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.rs_solve(prob, one)
+        samples.append(time.perf_counter() - t0)
+    t1 = statistics.median(samples)
+    t_iter = max((t3[0] - t1) / 2.0, 1e-9)
+    t_solve = max(t1 - t_iter, 0.0) + iters * t_iter
+    value = 1.0 / t_solve
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_solve, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": config(args.n, "cpu"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": (f"oracle/restate.c MG-PCG (the reference's CPU path has no 3D "
+                                    f"divergence-form MG-PCG), {cores} OpenMP threads; one converged solve "
+                                    f"({iters} iterations, {t_full:.1f}s) in warm-up, each step = setup + 1 "
+                                    f"iteration, solve = setup + {iters} iterations")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    from pde_solver_b200 import abi, synthetic
+    from pde_solver_b200.problem import default_options
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    lib = abi.load()
+
+    n = args.n
+    prob = synthetic.varcoef_poisson_3d(n, seed=SEED + rank)
+    N = prob.n
+    opt = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400, device=local)
+    stream = torch.cuda.current_stream(device)
+    assert lib.pdeb200_set_stream(local, C.c_void_p(stream.cuda_stream)) == abi.OK
+
+    # ---- device-resident inputs
+    k_dev = torch.from_numpy(prob.k).to(device)
+    f_dev = torch.from_numpy(prob.f).to(device)
+    out_dev = torch.empty(N, dtype=torch.float64, device=device)
+    import copy
+
+    dprob = copy.copy(prob)
+    dprob.k, dprob.f = None, None
+    dprob.mem_space = abi.MEM_DEVICE
+    dprob.k_dev, dprob.f_dev = k_dev.data_ptr(), f_dev.data_ptr()
+    cdev = dprob.to_c()
+
+    def solve_dev():
+        rep = abi.Report()
+        st = lib.pdeb200_solve(C.byref(cdev), C.byref(opt), C.c_void_p(out_dev.data_ptr()), C.byref(rep))
+        if st != abi.OK:
+            raise RuntimeError(f"solve failed: {st} {rep.message.decode()}")
+        return rep
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.warmup):
+        rep = solve_dev()
+    iters = rep.iterations
+    rel = rep.rel_residual
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    launches = 0
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rep = solve_dev()
+        launches += rep.kernel_launches
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- end to end through the same C-ABI call with pinned host buffers
+    k_host = torch.from_numpy(prob.k).pin_memory()
+    f_host = torch.from_numpy(prob.f).pin_memory()
+    out_host = torch.empty(N, dtype=torch.float64).pin_memory()
+    hprob = copy.copy(prob)
+    hprob.k, hprob.f = None, None
+    ch = hprob.to_c()
+    ch.k = C.cast(C.c_void_p(k_host.data_ptr()), C.POINTER(C.c_double))
+    ch.f = C.cast(C.c_void_p(f_host.data_ptr()), C.POINTER(C.c_double))
+
+    def solve_host():
+        rep = abi.Report()
+        st = lib.pdeb200_solve(C.byref(ch), C.byref(opt), C.c_void_p(out_host.data_ptr()), C.byref(rep))
+        if st != abi.OK:
+            raise RuntimeError(f"solve failed: {st} {rep.message.decode()}")
+        return rep
+
+    solve_host()
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        solve_host()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = e2.elapsed_time(e3)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * args.steps / (ms_e2e / 1e3)
+    ok_host = np.allclose(out_host.numpy(), out_dev.cpu().numpy(), rtol=0, atol=1e-12 * float(out_dev.abs().max()))
+
+    # ---- live per-kernel roofline (events around each finest-level launch)
+    lib.pdeb200_profile_enable(local, 1)
+    for _ in range(2):
+        solve_dev()
+    stats = (abi.KernelStat * 32)()
+    cnt = lib.pdeb200_profile_read(local, stats, 32)
+    lib.pdeb200_profile_enable(local, 0)
+    kern = []
+    for q in range(min(cnt, 32)):
+        s = stats[q]
+        if s.launches:
+            kern.append({"name": s.name.decode(), "launches": int(s.launches), "total_ms": s.total_ms,
+                         "avg_us": 1e3 * s.total_ms / s.launches, "bytes": s.bytes_per_launch,
+                         "gbs": s.bytes_per_launch / (s.total_ms / s.launches / 1e3) / 1e9})
+    kern.sort(key=lambda d: -d["total_ms"])
+    peak, peak_kind = peaks()
+    top = kern[0] if kern else None
+    roofline = None
+    if top:
+        traffic = ncu_traffic(top["name"])
+        roofline = {"bound": "hbm", "kernel": top["name"], "achieved": round(top["gbs"], 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(top["gbs"] / peak, 4), "peak_source": peak_kind,
+                    "traffic": traffic, "algorithmic_bytes_per_launch": top["bytes"],
+                    "avg_launch_us": round(top["avg_us"], 2),
+                    "kernels": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in d.items()}
+                                for d in kern[:8]]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded, generated on the host)",
+        "config": config(n, "inputs larger than L2 (k, f, x, r, p, q: 136 MB each)"),
+        "iterations": iters, "rel_residual": rel,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8,
+                "matches_device_result": bool(ok_host)},
+        "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_sample(prob, iters)
+        except Exception as exc:  # the baseline never blocks the GPU line
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {exc}"}
+    lib.pdeb200_set_stream(local, None)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

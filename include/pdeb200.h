@@ -212,6 +212,24 @@ void pdeb200_default_options(pdeb200_options* opt);
 /* Frees every cached workspace of every device context. */
 void pdeb200_release_all(void);
 
+/* Launch stream (a cudaStream_t passed as void*) of every later call on
+ * `device`; NULL restores the library's own non-blocking stream. Lets a host
+ * that owns a stream (torch, a serving loop) order and time the solves on it. */
+pdeb200_status pdeb200_set_stream(int32_t device, void* stream);
+
+/* Per-kernel device-time accounting: while enabled, each finest-level launch
+ * of the hot kernels is bracketed by CUDA events on its launch stream. */
+typedef struct {
+  char name[48];
+  int64_t launches;
+  double total_ms;          /* summed event-measured durations */
+  double bytes_per_launch;  /* algorithmic bytes of one launch (finest level) */
+} pdeb200_kernel_stat;
+
+void pdeb200_profile_enable(int32_t device, int32_t on);
+/* Copies up to max_stats entries; returns the number of kernels recorded. */
+int32_t pdeb200_profile_read(int32_t device, pdeb200_kernel_stat* stats, int32_t max_stats);
+
 /* ---- steady solve ----------------------------------------------------- */
 
 /* Replaces SolvePDECuda's dispatch (src/backends/cuda/CudaSolve.cu:31-64) and

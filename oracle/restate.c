@@ -1024,6 +1024,100 @@ static void rbgs_color(const Grid* g, const double* b, double* x, int color) {
       }
 }
 
+/* Homogeneous closure extension of a correction field: boundary nodes take
+ * c1 * (inward neighbour) in the reference's phase order (x, y, z faces),
+ * Dirichlet nodes 0. Ext is the map the folded system eliminates, so
+ * interpolating Ext(x_c) carries Neumann/Robin corrections to the faces. */
+static void ext_apply(const Grid* g, double* x) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  double c0, c1;
+  for (int f = LEFT; f <= BACK; ++f) {
+    if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
+                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
+          if (on) x[ID(g, i, j, k)] = 0.0;
+        }
+  }
+  for (int f = LEFT; f <= BACK; ++f) {
+    if (!face_active(g, f) || face_kind(g, f) == PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          int on = 0, ii = i, jj = j, kk = k;
+          if (f == LEFT && i == 0) { on = 1; ii = 1; }
+          if (f == RIGHT && i == nx - 1) { on = 1; ii = nx - 2; }
+          if (f == BOTTOM && j == 0) { on = 1; jj = 1; }
+          if (f == TOP && j == ny - 1) { on = 1; jj = ny - 2; }
+          if (f == FRONT && k == 0) { on = 1; kk = 1; }
+          if (f == BACK && k == nz - 1) { on = 1; kk = nz - 2; }
+          if (!on) continue;
+          face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
+          x[ID(g, i, j, k)] = c1 * x[ID(g, ii, jj, kk)];
+        }
+  }
+  for (int f = LEFT; f <= BACK; ++f) {
+    if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
+                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
+          if (on) x[ID(g, i, j, k)] = 0.0;
+        }
+  }
+}
+
+/* Transpose of ext_apply: Dirichlet nodes zeroed, then the Neumann/Robin
+ * phases in reverse (z, y, x): y[inward] += c1*y[b], y[b] = 0. */
+static void ext_transpose(const Grid* g, double* y) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  double c0, c1;
+  for (int f = LEFT; f <= BACK; ++f) {
+    if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
+                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
+          if (on) y[ID(g, i, j, k)] = 0.0;
+        }
+  }
+  for (int f = BACK; f >= LEFT; --f) {
+    if (!face_active(g, f) || face_kind(g, f) == PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          int on = 0, ii = i, jj = j, kk = k;
+          if (f == LEFT && i == 0) { on = 1; ii = 1; }
+          if (f == RIGHT && i == nx - 1) { on = 1; ii = nx - 2; }
+          if (f == BOTTOM && j == 0) { on = 1; jj = 1; }
+          if (f == TOP && j == ny - 1) { on = 1; jj = ny - 2; }
+          if (f == FRONT && k == 0) { on = 1; kk = 1; }
+          if (f == BACK && k == nz - 1) { on = 1; kk = nz - 2; }
+          if (!on) continue;
+          face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
+          y[ID(g, ii, jj, kk)] += c1 * y[ID(g, i, j, k)];
+          y[ID(g, i, j, k)] = 0.0;
+        }
+  }
+  for (int f = LEFT; f <= BACK; ++f) {
+    if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
+                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
+          if (on) y[ID(g, i, j, k)] = 0.0;
+        }
+  }
+}
+
+static int g_mg_boundary_transfer = 1;
+void rs_set_mg_boundary_transfer(int on) { g_mg_boundary_transfer = on; }
+
 static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coarse_iters) {
   Grid* g = &lv[l].g;
   double *x = lv[l].x, *b = lv[l].b;
@@ -1042,28 +1136,37 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   /* r = b - A x */
   folded_apply(g, x, lv[l].r);
   for (long q = 0; q < g->n; ++q) lv[l].r[q] = b[q] - lv[l].r[q];
-  /* full weighting r -> coarse b (tensor [1/4,1/2,1/4]), interior coarse nodes only */
+  /* full weighting r -> coarse b (tensor [1/4,1/2,1/4]) at every coarse node
+   * (in-range fine neighbours), then the transpose of the boundary extension
+   * folds the boundary-node values into the interior: R = Ext^T P^T / 2^dim. */
   Grid* c = &lv[l + 1].g;
   double* bc = lv[l + 1].b;
   memset(bc, 0, sizeof(double) * c->n);
-  const int kc0 = c->dim == 3 ? 1 : 0, kc1 = c->dim == 3 ? c->nz - 1 : 1;
+  const int all = g_mg_boundary_transfer;
+  const int kc0 = c->dim == 3 ? (all ? 0 : 1) : 0, kc1 = c->dim == 3 ? (all ? c->nz : c->nz - 1) : 1;
+  const int ic0 = all ? 0 : 1, ic1 = all ? c->nx : c->nx - 1, jc0 = all ? 0 : 1, jc1 = all ? c->ny : c->ny - 1;
   const double wt[3] = {0.25, 0.5, 0.25};
   for (int K = kc0; K < kc1; ++K)
-    for (int J = 1; J < c->ny - 1; ++J)
-      for (int I = 1; I < c->nx - 1; ++I) {
+    for (int J = jc0; J < jc1; ++J)
+      for (int I = ic0; I < ic1; ++I) {
         double acc = 0.0;
         const int dk0 = c->dim == 3 ? -1 : 0, dk1 = c->dim == 3 ? 1 : 0;
         for (int dk = dk0; dk <= dk1; ++dk)
           for (int dj = -1; dj <= 1; ++dj)
             for (int di = -1; di <= 1; ++di) {
+              const int fi = 2 * I + di, fj = 2 * J + dj, fk = c->dim == 3 ? 2 * K + dk : 0;
+              if (fi < 0 || fi >= g->nx || fj < 0 || fj >= g->ny || fk < 0 || fk >= g->nz) continue;
               const double w = wt[di + 1] * wt[dj + 1] * (c->dim == 3 ? wt[dk + 1] : 1.0);
-              acc += w * lv[l].r[ID(g, 2 * I + di, 2 * J + dj, c->dim == 3 ? 2 * K + dk : 0)];
+              acc += w * lv[l].r[ID(g, fi, fj, fk)];
             }
         bc[ID(c, I, J, K)] = acc;
       }
+  if (all) ext_transpose(c, bc);
   mg_vcycle_folded(lv, L, l + 1, pre, post, coarse_iters);
-  /* trilinear prolongation-add of the coarse correction (coarse boundary is 0) */
-  const double* xc = lv[l + 1].x;
+  /* trilinear prolongation-add of the coarse correction, extended to the
+   * coarse boundary by the homogeneous closures */
+  double* xc = lv[l + 1].x;
+  if (g_mg_boundary_transfer) ext_apply(c, xc);
   const int kf0 = g->dim == 3 ? 1 : 0, kf1 = g->dim == 3 ? g->nz - 1 : 1;
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = kf0; k < kf1; ++k)

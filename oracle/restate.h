@@ -32,6 +32,7 @@ int rs_folded_apply(const pdeb200_problem* prob, const double* x, double* y);
 int rs_fill_boundary(const pdeb200_problem* prob, double* grid);
 void rs_set_threads(int n);
 long rs_sizeof(int which);
+void rs_set_mg_boundary_transfer(int on);
 
 #ifdef __cplusplus
 }

@@ -149,6 +149,15 @@ class ProjectionReport(C.Structure):
     ]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 48),
+        ("launches", C.c_int64),
+        ("total_ms", C.c_double),
+        ("bytes_per_launch", C.c_double),
+    ]
+
+
 FRAME_CB = C.CFUNCTYPE(C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -182,6 +191,12 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_project_velocity.argtypes = [
         C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(ProjectionOptions), P(ProjectionReport)]
+    lib.pdeb200_set_stream.restype = C.c_int32
+    lib.pdeb200_set_stream.argtypes = [C.c_int32, C.c_void_p]
+    lib.pdeb200_profile_enable.restype = None
+    lib.pdeb200_profile_enable.argtypes = [C.c_int32, C.c_int32]
+    lib.pdeb200_profile_read.restype = C.c_int32
+    lib.pdeb200_profile_read.argtypes = [C.c_int32, P(KernelStat), C.c_int32]
     return lib
 
 

@@ -81,9 +81,27 @@ class Buf {
   cudaStream_t s_ = nullptr;
 };
 
+struct ProfPending {
+  const char* name;
+  cudaEvent_t a, b;
+  double bytes;
+};
+
+struct ProfStat {
+  std::string name;
+  long long launches = 0;
+  double total_ms = 0.0;
+  double bytes = 0.0;
+};
+
 struct Context {
   int dev = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // launch stream in use
+  cudaStream_t own_stream = nullptr;  // the library's own stream
+  bool prof = false;
+  std::vector<ProfPending> pending;
+  std::vector<ProfStat> stats;
+  std::vector<cudaEvent_t> evpool;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   Ctl* d_ctl = nullptr;     // device control block
   Ctl* h_ctl = nullptr;     // pinned mirror
@@ -96,11 +114,67 @@ struct Context {
   std::mutex mu;
   long long launches = 0;
 
+  cudaEvent_t ev_get() {
+    if (!evpool.empty()) {
+      cudaEvent_t e = evpool.back();
+      evpool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    PDEB_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+  // accumulate pending kernel timings (after the stream has been synchronised)
+  void prof_flush() {
+    for (auto& p : pending) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+        ProfStat* st = nullptr;
+        for (auto& s : stats)
+          if (s.name == p.name && s.bytes == p.bytes) st = &s;
+        if (!st) {
+          stats.push_back(ProfStat{p.name, 0, 0.0, p.bytes});
+          st = &stats.back();
+        }
+        st->launches += 1;
+        st->total_ms += ms;
+      }
+      evpool.push_back(p.a);
+      evpool.push_back(p.b);
+    }
+    pending.clear();
+  }
+
   RedSlot slot(int which = 0) const {
     return RedSlot{d_partials + (size_t)which * max_blocks * kMaxRed, d_tickets + which, d_redout + which * kMaxRed};
   }
   void count(int n = 1) { launches += n; }
 };
+
+// Brackets one launch with events on the launch stream while profiling is on.
+struct ProfScope {
+  Context* c;
+  const char* name;
+  double bytes;
+  cudaEvent_t a = nullptr;
+  ProfScope(Context* ctx, const char* n, double b, bool on) : c(ctx), name(n), bytes(b) {
+    if (c->prof && on) {
+      a = c->ev_get();
+      PDEB_CUDA(cudaEventRecord(a, c->stream));
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEvent_t b = c->ev_get();
+      cudaEventRecord(b, c->stream);
+      c->pending.push_back(ProfPending{name, a, b, bytes});
+    }
+  }
+};
+
+inline double interior_dofs(const GridDev& g) {
+  return double(g.nx - 2) * double(g.ny - 2) * double(g.dim == 3 ? g.nz - 2 : 1);
+}
 
 Context* get_context(int dev);  // throws StatusFailure / CudaFailure
 void release_contexts();

@@ -421,8 +421,74 @@ __global__ void k_fill(long long n, T* __restrict__ dst, T v, const Ctl* ctl) {
 
 // ------------------------------------------------------------ multigrid
 
-// Full weighting (tensor [1/4,1/2,1/4]) of the fine residual onto interior
-// coarse nodes, n_c = (n_f+1)/2 (multigrid.cpp:14-36 in 2D, trilinear in 3D).
+// Homogeneous closure chain of a boundary node: the folded system eliminates
+// boundary node b through u_b = c0 + c1*u_inward, applied in the reference's
+// phase order (x, y, z faces; the last phase containing b writes it). For a
+// correction field (c0 = 0) the value at b is coef * u(end), where `end` is the
+// interior node the chain reaches. Nodes on a Dirichlet face have coef 0.
+// (i,j,k) is moved to `end`; returns coef.
+__device__ __forceinline__ double ext_chain(const GridDev& g, int& i, int& j, int& k) {
+  {
+    const bool on[6] = {i == 0, i == g.nx - 1, j == 0, j == g.ny - 1, g.dim == 3 && k == 0,
+                        g.dim == 3 && k == g.nz - 1};
+    for (int f = 0; f < 6; ++f)
+      if (on[f] && g.face[f].active && g.face[f].kind == kDirichlet) return 0.0;
+  }
+  double coef = 1.0;
+  for (int depth = 0; depth < 3; ++depth) {
+    int f = -1;
+    if (g.dim == 3 && k == g.nz - 1) f = kBack;
+    else if (g.dim == 3 && k == 0) f = kFront;
+    else if (j == g.ny - 1) f = kTop;
+    else if (j == 0) f = kBottom;
+    else if (i == g.nx - 1) f = kRight;
+    else if (i == 0) f = kLeft;
+    if (f < 0) break;
+    const int loc = f <= kRight ? j + g.ny * k : (f <= kTop ? i + g.nx * k : i + g.nx * j);
+    coef *= g.face[f].c1.at(loc);
+    if (f == kLeft) i = 1;
+    else if (f == kRight) i = g.nx - 2;
+    else if (f == kBottom) j = 1;
+    else if (f == kTop) j = g.ny - 2;
+    else if (f == kFront) k = 1;
+    else k = g.nz - 2;
+  }
+  return coef;
+}
+
+// Full weighting (tensor [1/4,1/2,1/4]) of the fine residual at coarse node
+// (I,J,K), boundary coarse nodes included (fine neighbours outside the grid
+// do not exist; fine boundary values of the residual are zero).
+template <typename T>
+__device__ __forceinline__ double full_weight(const GridDev& gf, const GridDev& gc, const T* __restrict__ rf, int I,
+                                              int J, int K) {
+  const double w[3] = {0.25, 0.5, 0.25};
+  const int fi = 2 * I, fj = 2 * J, fk = gc.dim == 3 ? 2 * K : 0;
+  double acc = 0.0;
+  const int dk0 = gc.dim == 3 ? -1 : 0, dk1 = gc.dim == 3 ? 1 : 0;
+  for (int dk = dk0; dk <= dk1; ++dk) {
+    const int kk = fk + dk;
+    if (kk < 0 || kk >= gf.nz) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int jj = fj + dj;
+      if (jj < 0 || jj >= gf.ny) continue;
+      for (int di = -1; di <= 1; ++di) {
+        const int ii = fi + di;
+        if (ii < 0 || ii >= gf.nx) continue;
+        acc += w[di + 1] * w[dj + 1] * (gc.dim == 3 ? w[dk + 1] : 1.0) *
+               double(rf[((long long)kk * gf.ny + jj) * gf.nx + ii]);
+      }
+    }
+  }
+  return acc;
+}
+
+// Restriction R = Ext^T P^T / 2^dim onto interior coarse nodes: full weighting
+// at the node itself plus, for nodes next to a Neumann/Robin face, the full
+// weighting at every boundary node whose closure chain ends here, times the
+// chain's coefficient. The transpose of the extended prolongation below, so
+// the V-cycle stays a symmetric preconditioner. Each coarse node gathers its
+// own value: race free.
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_restrict(GridDev gf, GridDev gc, const T* __restrict__ rf,
                                                        TC* __restrict__ bc, const Ctl* ctl) {
@@ -432,31 +498,42 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict(GridDev gf, GridDev gc, c
   int K0, K1;
   column_range(gc, K0, K1);
   if (!(I >= 1 && I <= gc.nx - 2 && J >= 1 && J <= gc.ny - 2)) return;
-  const double w[3] = {0.25, 0.5, 0.25};
+  const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
+  const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
   for (int K = K0; K < K1; ++K) {
+    const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
     double acc = 0.0;
-    const int kf = gc.dim == 3 ? 2 * K : 0;
-    const long long base = ((long long)kf * gf.ny + 2 * J) * gf.nx + 2 * I;
-    if (gc.dim == 3) {
-#pragma unroll
-      for (int dk = -1; dk <= 1; ++dk)
-#pragma unroll
-        for (int dj = -1; dj <= 1; ++dj)
-#pragma unroll
-          for (int di = -1; di <= 1; ++di)
-            acc += w[di + 1] * w[dj + 1] * w[dk + 1] * double(rf[base + dk * gf.sxy + dj * gf.nx + di]);
-    } else {
-#pragma unroll
-      for (int dj = -1; dj <= 1; ++dj)
-#pragma unroll
-        for (int di = -1; di <= 1; ++di) acc += w[di + 1] * w[dj + 1] * double(rf[base + dj * gf.nx + di]);
-    }
+    for (int dk = dzl; dk <= dzh; ++dk)
+      for (int dj = dyl; dj <= dyh; ++dj)
+        for (int di = dxl; di <= dxh; ++di) {
+          if (di == 0 && dj == 0 && dk == 0) {
+            acc += full_weight<T>(gf, gc, rf, I, J, K);
+            continue;
+          }
+          int ci = I + di, cj = J + dj, ck = K + dk;
+          const double coef = ext_chain(gc, ci, cj, ck);
+          if (coef != 0.0 && ci == I && cj == J && ck == K) acc += coef * full_weight<T>(gf, gc, rf, I + di, J + dj, K + dk);
+        }
     bc[((long long)K * gc.ny + J) * gc.nx + I] = TC(acc);
   }
 }
 
-// Trilinear (bilinear in 2D) prolongation of the coarse correction added to
-// the fine interior (multigrid.cpp:38-67); the coarse boundary is zero.
+__device__ __forceinline__ long long cidx(const GridDev& g, int i, int j, int k) {
+  return ((long long)k * g.ny + j) * g.nx + i;
+}
+
+// coarse correction value at any coarse node, boundary nodes by the
+// homogeneous closure chain
+template <typename TC>
+__device__ __forceinline__ double ext_value(const GridDev& gc, const TC* __restrict__ xc, int I, int J, int K) {
+  const bool bd = I == 0 || I == gc.nx - 1 || J == 0 || J == gc.ny - 1 || (gc.dim == 3 && (K == 0 || K == gc.nz - 1));
+  if (!bd) return double(xc[cidx(gc, I, J, K)]);
+  const double coef = ext_chain(gc, I, J, K);
+  return coef == 0.0 ? 0.0 : coef * double(xc[cidx(gc, I, J, K)]);
+}
+
+// Trilinear (bilinear in 2D) prolongation of the coarse correction, extended
+// to the coarse boundary through the closures, added to the fine interior.
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc, const TC* __restrict__ xc,
                                                           T* __restrict__ xf, const Ctl* ctl) {
@@ -467,13 +544,21 @@ __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc
   column_range(gf, k0, k1);
   if (!(i >= 1 && i <= gf.nx - 2 && j >= 1 && j <= gf.ny - 2)) return;
   const int I0 = i >> 1, I1 = (i + 1) >> 1, J0 = j >> 1, J1 = (j + 1) >> 1;
+  const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
   for (int k = k0; k < k1; ++k) {
     const int K0 = gf.dim == 3 ? k >> 1 : 0, K1 = gf.dim == 3 ? (k + 1) >> 1 : 0;
-    const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
-    const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
-    const double v = 0.125 * (double(xc[a0 + r0 + I0]) + double(xc[a0 + r0 + I1]) + double(xc[a0 + r1 + I0]) +
-                              double(xc[a0 + r1 + I1]) + double(xc[a1 + r0 + I0]) + double(xc[a1 + r0 + I1]) +
-                              double(xc[a1 + r1 + I0]) + double(xc[a1 + r1 + I1]));
+    double v;
+    if (!xy_edge && !(gf.dim == 3 && (K0 == 0 || K1 == gc.nz - 1))) {
+      const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
+      const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
+      v = 0.125 * (double(xc[a0 + r0 + I0]) + double(xc[a0 + r0 + I1]) + double(xc[a0 + r1 + I0]) +
+                   double(xc[a0 + r1 + I1]) + double(xc[a1 + r0 + I0]) + double(xc[a1 + r0 + I1]) +
+                   double(xc[a1 + r1 + I0]) + double(xc[a1 + r1 + I1]));
+    } else {
+      v = 0.125 * (ext_value(gc, xc, I0, J0, K0) + ext_value(gc, xc, I1, J0, K0) + ext_value(gc, xc, I0, J1, K0) +
+                   ext_value(gc, xc, I1, J1, K0) + ext_value(gc, xc, I0, J0, K1) + ext_value(gc, xc, I1, J0, K1) +
+                   ext_value(gc, xc, I0, J1, K1) + ext_value(gc, xc, I1, J1, K1));
+    }
     const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
     xf[id] = T(double(xf[id]) + v);
   }

@@ -34,7 +34,8 @@ Context* get_context(int dev) {
     PDEB_CUDA(cudaGetDeviceProperties(&prop, dev));
     c->name = prop.name;
     c->num_sms = prop.multiProcessorCount;
-    PDEB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PDEB_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
     PDEB_CUDA(cudaEventCreate(&c->ev0));
     PDEB_CUDA(cudaEventCreate(&c->ev1));
     PDEB_CUDA(cudaMalloc(&c->d_ctl, sizeof(Ctl)));
@@ -68,7 +69,8 @@ void release_contexts() {
     cudaFree(c->d_redout);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
-    cudaStreamDestroy(c->stream);
+    for (auto e : c->evpool) cudaEventDestroy(e);
+    cudaStreamDestroy(c->own_stream);
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, c->dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     c.reset();
@@ -406,6 +408,44 @@ void pdeb200_default_options(pdeb200_options* o) {
 
 void pdeb200_release_all(void) { release_contexts(); }
 
+pdeb200_status pdeb200_set_stream(int32_t device, void* stream) {
+  return guarded(nullptr, [&]() -> pdeb200_status {
+    Context* ctx = get_context(device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return PDEB200_OK;
+  });
+}
+
+void pdeb200_profile_enable(int32_t device, int32_t on) {
+  guarded(nullptr, [&]() -> pdeb200_status {
+    Context* ctx = get_context(device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->prof = on != 0;
+    if (on) ctx->stats.clear();
+    return PDEB200_OK;
+  });
+}
+
+int32_t pdeb200_profile_read(int32_t device, pdeb200_kernel_stat* stats, int32_t max_stats) {
+  int32_t count = 0;
+  guarded(nullptr, [&]() -> pdeb200_status {
+    Context* ctx = get_context(device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    count = (int32_t)ctx->stats.size();
+    for (int32_t q = 0; q < count && q < max_stats && stats; ++q) {
+      std::memset(&stats[q], 0, sizeof(stats[q]));
+      std::strncpy(stats[q].name, ctx->stats[q].name.c_str(), sizeof(stats[q].name) - 1);
+      stats[q].launches = ctx->stats[q].launches;
+      stats[q].total_ms = ctx->stats[q].total_ms;
+      stats[q].bytes_per_launch = ctx->stats[q].bytes;
+    }
+    return PDEB200_OK;
+  });
+  return count;
+}
+
 pdeb200_status pdeb200_solve(const pdeb200_problem* prob, const pdeb200_options* opt, double* out_grid,
                              pdeb200_report* report) {
   const double t0 = now_ms();
@@ -432,6 +472,7 @@ pdeb200_status pdeb200_solve(const pdeb200_problem* prob, const pdeb200_options*
       PDEB_CUDA(cudaMemcpyAsync(out_grid, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
     PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
     PDEB_CUDA(cudaGetLastError());
+    ctx->prof_flush();
     if (report) report->kernel_launches = (int32_t)ctx->launches;
     return s;
   });

@@ -141,15 +141,28 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
   k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 1);
   ctx->count(2);
   const dim3 grid = stencil_grid(g), block = stencil_block();
+  const double dofs = interior_dofs(g);
   auto iterate = [&](int) {
-    k_apply_folded<Coef, double, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(),
-                                                                                 PostAlpha{ctx->d_ctl}, ctx->d_ctl);
-    k_cg_xr<double, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, d_x, r, p, q, ctx->slot(), PostRRRel{ctx->d_ctl},
-                                                            ctx->d_ctl);
+    {
+      ProfScope ps(ctx, "apply_dot", dofs * 24.0, true);
+      k_apply_folded<Coef, double, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(),
+                                                                                   PostAlpha{ctx->d_ctl}, ctx->d_ctl);
+    }
+    {
+      ProfScope ps(ctx, "cg_update_xr", dofs * 48.0, true);
+      k_cg_xr<double, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, d_x, r, p, q, ctx->slot(), PostRRRel{ctx->d_ctl},
+                                                              ctx->d_ctl);
+    }
     ctx->count(2);
     H.vcycle(ctx, r, ctx->d_ctl);
-    k_dot<double, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{ctx->d_ctl}, ctx->d_ctl);
-    k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 0);
+    {
+      ProfScope ps(ctx, "dot", dofs * 16.0, true);
+      k_dot<double, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{ctx->d_ctl}, ctx->d_ctl);
+    }
+    {
+      ProfScope ps(ctx, "cg_update_p", dofs * 24.0, true);
+      k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 0);
+    }
     ctx->count(2);
   };
   pdeb200_status st = drive(ctx, o, max_iter + 1, iterate, false);

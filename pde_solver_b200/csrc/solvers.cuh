@@ -389,11 +389,16 @@ struct Hierarchy {
     }
   }
 
-  void smooth(Context* ctx, const Level& L, const T* b, int sweeps, bool reverse, const Ctl* ctl) {
+  // one colour pass: 16 algorithmic bytes per interior node in FP64 (a full
+  // red+black sweep reads u, f, k and writes u once: 32 B/DOF)
+  void smooth(Context* ctx, const Level& L, const T* b, int sweeps, bool reverse, const Ctl* ctl, bool fine) {
     const dim3 grid = stencil_grid(L.g), block = stencil_block();
+    const double bytes = interior_dofs(L.g) * 2.0 * sizeof(T);
     for (int s = 0; s < sweeps; ++s) {
-      k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, reverse ? 1 : 0, ctl);
-      k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, reverse ? 0 : 1, ctl);
+      for (int half = 0; half < 2; ++half) {
+        ProfScope ps(ctx, "rbgs_color_pass", bytes, fine);
+        k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, (reverse ? 1 : 0) ^ half, ctl);
+      }
       ctx->count(2);
     }
   }
@@ -401,26 +406,40 @@ struct Hierarchy {
   void level(Context* ctx, int l, const T* rhs0, const Ctl* ctl) {
     Level& L = levels[l];
     const T* b = l == 0 ? rhs0 : L.b;
-    vfill<T>(ctx, L.g.n, L.x, T(0), ctl);
+    const bool fine = l == 0;
+    const double dofs = interior_dofs(L.g);
+    {
+      ProfScope ps(ctx, "zero_fill", dofs * sizeof(T), fine);
+      vfill<T>(ctx, L.g.n, L.x, T(0), ctl);
+    }
     if (l == (int)levels.size() - 1) {
       if (L.g.n <= 65536) {
         k_coarse_solve<Coef, T, T><<<1, 256, 0, ctx->stream>>>(L.g, L.cf, b, L.x, coarse_iters, ctl);
         ctx->count();
       } else {
-        smooth(ctx, L, b, coarse_iters, false, ctl);
+        smooth(ctx, L, b, coarse_iters, false, ctl, fine);
       }
       return;
     }
-    smooth(ctx, L, b, pre, false, ctl);
-    k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(
-        L.g, L.cf, L.x, b, L.r, RedSlot{}, NoPost{}, ctl);
+    smooth(ctx, L, b, pre, false, ctl, fine);
+    {
+      ProfScope ps(ctx, "residual", dofs * 4.0 * sizeof(T), fine);
+      k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(
+          L.g, L.cf, L.x, b, L.r, RedSlot{}, NoPost{}, ctl);
+    }
     Level& C = levels[l + 1];
-    k_restrict<T, T><<<stencil_grid(C.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+    {
+      ProfScope ps(ctx, "restrict", dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)), fine);
+      k_restrict<T, T><<<stencil_grid(C.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+    }
     ctx->count(2);
     level(ctx, l + 1, rhs0, ctl);
-    k_prolong_add<T, T><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.x, L.x, ctl);
+    {
+      ProfScope ps(ctx, "prolong_add", dofs * sizeof(T) * (2.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)), fine);
+      k_prolong_add<T, T><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.x, L.x, ctl);
+    }
     ctx->count();
-    smooth(ctx, L, b, post, true, ctl);
+    smooth(ctx, L, b, post, true, ctl, fine);
   }
 
   // z = M rhs0, result in levels[0].x
