@@ -328,19 +328,20 @@ def main():
     lib.pdeb200_profile_enable(local, 1)
     for _ in range(2):
         solve_dev()
-    stats = (abi.KernelStat * 32)()
-    cnt = lib.pdeb200_profile_read(local, stats, 32)
+    stats = (abi.KernelStat * 128)()
+    cnt = lib.pdeb200_profile_read(local, stats, 128)
     lib.pdeb200_profile_enable(local, 0)
     kern = []
-    for q in range(min(cnt, 32)):
+    for q in range(min(cnt, 128)):
         s = stats[q]
         if s.launches:
             kern.append({"name": s.name.decode(), "launches": int(s.launches), "total_ms": s.total_ms,
                          "avg_us": 1e3 * s.total_ms / s.launches, "bytes": s.bytes_per_launch,
                          "gbs": s.bytes_per_launch / (s.total_ms / s.launches / 1e3) / 1e9})
     kern.sort(key=lambda d: -d["total_ms"])
+    fine = [d for d in kern if d["name"].endswith("@L0")]
     peak, peak_kind = peaks()
-    top = kern[0] if kern else None
+    top = fine[0] if fine else (kern[0] if kern else None)
     roofline = None
     if top:
         traffic = ncu_traffic(top["name"])
@@ -349,7 +350,7 @@ def main():
                     "traffic": traffic, "algorithmic_bytes_per_launch": top["bytes"],
                     "avg_launch_us": round(top["avg_us"], 2),
                     "kernels": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in d.items()}
-                                for d in kern[:8]]}
+                                for d in kern[:16]]}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

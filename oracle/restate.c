@@ -926,8 +926,9 @@ static void fill_boundary(const Grid* g, double* u) {
 /* ---------------------------------------------------- MG hierarchy (B200) */
 
 /* Geometric hierarchy of the folded operator: vertex-centred coarsening
- * n_c = (n+1)/2 while every active dimension is odd and >= 5 (the rule of
- * multigrid.cpp:150-170), coarse k by injection, faces and h rediscretised. */
+ * n_c = (n+1)/2 while every active dimension is odd and >= 5 (the coarsening
+ * of multigrid.cpp:150-170, continued down to 3 nodes), coarse k by
+ * injection, faces and h rediscretised. */
 typedef struct {
   Grid g;
   pdeb200_problem p;
@@ -987,7 +988,6 @@ static int build_levels(const Grid* g0, int max_levels, Level* lv) {
     }
     c->p.f = NULL;
     ++L;
-    if (c->g.nx <= 5 || c->g.ny <= 5 || (c->g.dim == 3 && c->g.nz <= 5)) break;
   }
   for (int l = 0; l < L; ++l) {
     lv[l].x = calloc(lv[l].g.n, sizeof(double));

@@ -82,7 +82,7 @@ class Buf {
 };
 
 struct ProfPending {
-  const char* name;
+  std::string name;
   cudaEvent_t a, b;
   double bytes;
 };
@@ -152,13 +152,15 @@ struct Context {
 };
 
 // Brackets one launch with events on the launch stream while profiling is on.
+// Names carry the MG level ("rbgs_color_pass@L0"); level -1 = no level.
 struct ProfScope {
   Context* c;
-  const char* name;
+  std::string name;
   double bytes;
   cudaEvent_t a = nullptr;
-  ProfScope(Context* ctx, const char* n, double b, bool on) : c(ctx), name(n), bytes(b) {
-    if (c->prof && on) {
+  ProfScope(Context* ctx, const char* n, int level, double b) : c(ctx), bytes(b) {
+    if (c->prof) {
+      name = level >= 0 ? std::string(n) + "@L" + std::to_string(level) : std::string(n);
       a = c->ev_get();
       PDEB_CUDA(cudaEventRecord(a, c->stream));
     }
@@ -210,6 +212,11 @@ CoefConst make_const(double a, double b, double az, double c, double d, double d
 inline dim3 stencil_block() { return dim3(kBx, kBy, 1); }
 dim3 stencil_grid(const GridDev& g, int zchunk = 16);
 dim3 stencil_grid_full(const GridDev& g, int zchunk = 16);
+// z-chunking chosen for occupancy: about kTargetBlocks blocks, at least one
+// interior plane per thread
+dim3 stencil_grid_auto(const GridDev& g);
+// launch shape of the fused red-black sweep (64 x 8 column tiles)
+dim3 fused_grid(const GridDev& g);
 inline int vec_blocks(long long n, const Context* ctx) {
   long long b = (n + 255) / 256;
   long long cap = (long long)ctx->num_sms * 8;

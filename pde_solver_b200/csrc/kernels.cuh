@@ -157,6 +157,135 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
   }
 }
 
+// One full red-black Gauss-Seidel sweep in a single pass (colour `first`
+// updated first, then the other), reading x_in and writing x_out (distinct
+// buffers). The first colour only reads the other colour's old values
+// (x_in); the second colour reads the new first-colour values, which each
+// block recomputes on its tile plus a one-node halo and keeps in a 3-plane
+// shared-memory ring while marching in z. Halo values are computed from
+// x_in only, so every block gets identical numbers and the sweep is race free
+// and deterministic. One pass moves x, k and b once: half the traffic of two
+// colour passes. zero_in: x_in is identically zero (first sweep of a V-cycle
+// level), so it is not read.
+template <class Coef, typename T, typename TB>
+__device__ __forceinline__ T gs_update(const GridDev& g, const Coef& cf, const TB* __restrict__ b, int i, int j,
+                                       int k, long long id, T xp, T xm, T yp, T ym, T zp, T zm) {
+  Stencil<T> s = cf.template at<T>(g, id);
+  fold_faces<T>(g, i, j, k, s, nullptr);
+  return (T(b[id]) - nb_sum<T>(s, xp, xm, yp, ym, zp, zm, g.dim)) / s.c;
+}
+
+// Tile of the fused sweep: 64 x 8 columns, each thread owns two adjacent
+// x-columns (one of each colour on every plane); a ring of first-colour values
+// over the tile plus a one-node halo covers kSlab + 2 planes, and each barrier
+// phase handles kSlab planes so many loads are in flight per phase.
+constexpr int kFx = 2 * kBx;          // 64 columns
+constexpr int kHx = kFx + 2, kHy = kBy + 2;
+constexpr int kSlab = 4;
+constexpr int kRing = kSlab + 2;
+constexpr int kHalo = 2 * kHx + 2 * kBy;  // 148 border cells
+
+template <class Coef, typename T, typename TB>
+__global__ void __launch_bounds__(kBx* kBy) k_rbgs_fused(GridDev g, Coef cf, const TB* __restrict__ b,
+                                                         const T* __restrict__ xin, T* __restrict__ xout,
+                                                         int first, int zero_in, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  __shared__ T ring[kRing][kHy][kHx];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + kBx * ty;
+  const int i0 = blockIdx.x * kFx, j0 = blockIdx.y * kBy;
+  int k0, k1;
+  column_range(g, k0, k1);
+  if (k0 >= k1) return;
+  const bool is3 = g.dim == 3;
+  const int klo = is3 ? 1 : 0, khi = is3 ? g.nz - 2 : 0;
+  auto interior = [&](int ii, int jj, int kk) {
+    return ii >= 1 && ii <= g.nx - 2 && jj >= 1 && jj <= g.ny - 2 && kk >= klo && kk <= khi;
+  };
+  auto X = [&](int ii, int jj, int kk) -> T {
+    return zero_in ? T(0) : xin[((long long)kk * g.ny + jj) * g.nx + ii];
+  };
+  // first-colour update at a node from x_in (0 off the interior)
+  auto first_val = [&](int ii, int jj, int kk) -> T {
+    if (!interior(ii, jj, kk)) return T(0);
+    const long long id = ((long long)kk * g.ny + jj) * g.nx + ii;
+    const T zp = is3 ? X(ii, jj, kk + 1) : T(0);
+    const T zm = is3 ? X(ii, jj, kk - 1) : T(0);
+    return gs_update<Coef, T, TB>(g, cf, b, ii, jj, kk, id, X(ii + 1, jj, kk), X(ii - 1, jj, kk), X(ii, jj + 1, kk),
+                                  X(ii, jj - 1, kk), zp, zm);
+  };
+  auto slot = [&](int p) { return ((p % kRing) + kRing) % kRing; };
+  // border cell of this thread (tid < kHalo)
+  int hcol = -1, hrow = -1;
+  if (tid < kHalo) {
+    if (tid < kHx) {
+      hcol = tid;
+      hrow = 0;
+    } else if (tid < 2 * kHx) {
+      hcol = tid - kHx;
+      hrow = kHy - 1;
+    } else if (tid < 2 * kHx + kBy) {
+      hcol = 0;
+      hrow = 1 + (tid - 2 * kHx);
+    } else {
+      hcol = kHx - 1;
+      hrow = 1 + (tid - 2 * kHx - kBy);
+    }
+  }
+  const int jj = j0 + ty;
+  // first colour on plane p for the tile + halo; own first-colour nodes of
+  // planes in [k0,k1) are also stored to x_out
+  auto first_plane = [&](int p) {
+    const int sp = slot(p);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int ii = i0 + 2 * tx + c;
+      if (((ii + jj + p) & 1) != first) continue;
+      const T v = first_val(ii, jj, p);
+      ring[sp][ty + 1][2 * tx + c + 1] = v;
+      if (p >= k0 && p < k1 && interior(ii, jj, p)) xout[((long long)p * g.ny + jj) * g.nx + ii] = v;
+    }
+    if (hcol >= 0) {
+      const int gi = i0 - 1 + hcol, gj = j0 - 1 + hrow;
+      if (((gi + gj + p) & 1) == first) ring[sp][hrow][hcol] = first_val(gi, gj, p);
+    }
+  };
+  auto second_plane = [&](int q) {
+    const int sq = slot(q);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int ii = i0 + 2 * tx + c;
+      if (((ii + jj + q) & 1) == first || !interior(ii, jj, q)) continue;
+      const int col = 2 * tx + c + 1, row = ty + 1;
+      const T zp = is3 ? ring[slot(q + 1)][row][col] : T(0);
+      const T zm = is3 ? ring[slot(q - 1)][row][col] : T(0);
+      const long long id = ((long long)q * g.ny + jj) * g.nx + ii;
+      xout[id] = gs_update<Coef, T, TB>(g, cf, b, ii, jj, q, id, ring[sq][row][col + 1], ring[sq][row][col - 1],
+                                        ring[sq][row + 1][col], ring[sq][row - 1][col], zp, zm);
+    }
+  };
+  if (!is3) {
+    first_plane(0);
+    __syncthreads();
+    second_plane(0);
+    return;
+  }
+  first_plane(k0 - 1);
+  first_plane(k0);
+  for (int q0 = k0; q0 < k1; q0 += kSlab) {
+    const int qe = min(q0 + kSlab, k1);
+    // first colour for planes q0+1 .. qe (plane qe may lie past the chunk)
+#pragma unroll
+    for (int s = 1; s <= kSlab; ++s)
+      if (q0 + s <= qe) first_plane(q0 + s);
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kSlab; ++s)
+      if (q0 + s < qe) second_plane(q0 + s);
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------- full apply
 
 // y = L x with identity boundary rows: LinearOperator2D::Apply
@@ -165,8 +294,8 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
 template <class Coef, int NV, class Post>
 __global__ void __launch_bounds__(kBx* kBy) k_apply_full(GridDev g, Coef cf, const double* __restrict__ x,
                                                          double* __restrict__ y, RedSlot slot, Post post,
-                                                         const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+                                                         const Ctl* ctl, const double* __restrict__ w = nullptr) {
+  if (ctl_stopped(ctl)) return;
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
   // full z range (boundary planes included) split into chunks
@@ -188,7 +317,7 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_full(GridDev g, Coef cf, con
         v = x[id];
       }
       y[id] = v;
-      if constexpr (NV > 0) acc[0] += x[id] * v;
+      if constexpr (NV > 0) acc[0] += (w ? w[id] : x[id]) * v;
     }
   }
   if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
@@ -265,30 +394,44 @@ __device__ __forceinline__ int face_loc(const GridDev& g, int f, int i, int j, i
   return f <= kRight ? j + g.ny * k : (f <= kTop ? i + g.nx * k : i + g.nx * j);
 }
 
-__device__ __forceinline__ double boundary_final(const GridDev& g, const double* u, int i, int j, int k) {
-  // Dirichlet winner: back, front, top, bottom, right, left (reverse write order)
-  const bool on[6] = {i == 0, i == g.nx - 1, j == 0, j == g.ny - 1, g.dim == 3 && k == 0,
-                      g.dim == 3 && k == g.nz - 1};
-  for (int f = 5; f >= 0; --f)
-    if (on[f] && g.face[f].active && g.face[f].kind == kDirichlet) return g.face[f].val.at(face_loc(g, f, i, j, k));
+// dirichlet_last: the reference sequence ends with its Dirichlet pass (every
+// path except 2D Gauss-Seidel/SOR, which applies Dirichlet once before the
+// first sweep and only Neumann/Robin closures per iteration,
+// relaxation.cpp:66,135). Without it, a node on both kinds of face keeps the
+// Neumann/Robin value and a chain may end on a Dirichlet node.
+__device__ __forceinline__ double boundary_final(const GridDev& g, const double* u, int i, int j, int k,
+                                                 bool dirichlet_last = true) {
+  auto dirichlet_winner = [&](int ci, int cj, int ck, double* v) {
+    const bool on[6] = {ci == 0, ci == g.nx - 1, cj == 0, cj == g.ny - 1, g.dim == 3 && ck == 0,
+                        g.dim == 3 && ck == g.nz - 1};
+    for (int f = 5; f >= 0; --f)
+      if (on[f] && g.face[f].active && g.face[f].kind == kDirichlet) {
+        *v = g.face[f].val.at(face_loc(g, f, ci, cj, ck));
+        return true;
+      }
+    return false;
+  };
+  double dv;
+  if (dirichlet_last && dirichlet_winner(i, j, k, &dv)) return dv;
   int chain_f[3], chain_loc[3], cnt = 0;
   int ci = i, cj = j, ck = k;
   double base = 0.0;
   for (int depth = 0; depth < 4; ++depth) {
     const bool cb[6] = {ci == 0, ci == g.nx - 1, cj == 0, cj == g.ny - 1, g.dim == 3 && ck == 0,
                         g.dim == 3 && ck == g.nz - 1};
+    // the last Neumann/Robin phase containing the node writes it
     int f = -1;
     for (int q = 5; q >= 0; --q)
-      if (cb[q] && g.face[q].active) {
+      if (cb[q] && g.face[q].active && g.face[q].kind != kDirichlet) {
         f = q;
         break;
       }
     if (f < 0) {
-      base = u[((long long)ck * g.ny + cj) * g.nx + ci];
-      break;
-    }
-    if (g.face[f].kind == kDirichlet) {
-      base = g.face[f].val.at(face_loc(g, f, ci, cj, ck));
+      const bool bd = cb[0] || cb[1] || cb[2] || cb[3] || cb[4] || cb[5];
+      if (bd && dirichlet_winner(ci, cj, ck, &dv))
+        base = dv;
+      else
+        base = u[((long long)ck * g.ny + cj) * g.nx + ci];
       break;
     }
     chain_f[cnt] = f;
@@ -313,7 +456,7 @@ __device__ __forceinline__ double boundary_final(const GridDev& g, const double*
 
 // One thread per node of the six faces; a node shared by faces is written by
 // the first face (in face order) that contains it.
-static __global__ void k_fill_boundary(GridDev g, double* __restrict__ u, const Ctl* ctl) {
+static __global__ void k_fill_boundary(GridDev g, double* __restrict__ u, const Ctl* ctl, int dirichlet_last = 1) {
   if (ctl_skip(ctl)) return;
   const long long nxy = (long long)g.nx * g.ny;
   const long long nyz = (long long)g.ny * g.nz, nxz = (long long)g.nx * g.nz;
@@ -352,7 +495,7 @@ static __global__ void k_fill_boundary(GridDev g, double* __restrict__ u, const 
         break;
       }
     if (owner != f) continue;
-    u[((long long)k * g.ny + j) * g.nx + i] = boundary_final(g, u, i, j, k);
+    u[((long long)k * g.ny + j) * g.nx + i] = boundary_final(g, u, i, j, k, dirichlet_last != 0);
   }
 }
 
@@ -456,42 +599,60 @@ __device__ __forceinline__ double ext_chain(const GridDev& g, int& i, int& j, in
   return coef;
 }
 
+__device__ __forceinline__ long long cidx(const GridDev& g, int i, int j, int k) {
+  return ((long long)k * g.ny + j) * g.nx + i;
+}
+
 // Full weighting (tensor [1/4,1/2,1/4]) of the fine residual at coarse node
 // (I,J,K), boundary coarse nodes included (fine neighbours outside the grid
 // do not exist; fine boundary values of the residual are zero).
 template <typename T>
 __device__ __forceinline__ double full_weight(const GridDev& gf, const GridDev& gc, const T* __restrict__ rf, int I,
                                               int J, int K) {
-  const double w[3] = {0.25, 0.5, 0.25};
   const int fi = 2 * I, fj = 2 * J, fk = gc.dim == 3 ? 2 * K : 0;
   double acc = 0.0;
   const int dk0 = gc.dim == 3 ? -1 : 0, dk1 = gc.dim == 3 ? 1 : 0;
   for (int dk = dk0; dk <= dk1; ++dk) {
     const int kk = fk + dk;
     if (kk < 0 || kk >= gf.nz) continue;
+    const double wk = gc.dim == 3 ? (dk == 0 ? 0.5 : 0.25) : 1.0;
     for (int dj = -1; dj <= 1; ++dj) {
       const int jj = fj + dj;
       if (jj < 0 || jj >= gf.ny) continue;
-      for (int di = -1; di <= 1; ++di) {
-        const int ii = fi + di;
-        if (ii < 0 || ii >= gf.nx) continue;
-        acc += w[di + 1] * w[dj + 1] * (gc.dim == 3 ? w[dk + 1] : 1.0) *
-               double(rf[((long long)kk * gf.ny + jj) * gf.nx + ii]);
-      }
+      const double wjk = wk * (dj == 0 ? 0.5 : 0.25);
+      const long long row = ((long long)kk * gf.ny + jj) * gf.nx;
+      double rs = 0.0;
+      if (fi - 1 >= 0) rs += 0.25 * double(rf[row + fi - 1]);
+      rs += 0.5 * double(rf[row + fi]);
+      if (fi + 1 < gf.nx) rs += 0.25 * double(rf[row + fi + 1]);
+      acc += wjk * rs;
     }
   }
   return acc;
 }
 
-// Restriction R = Ext^T P^T / 2^dim onto interior coarse nodes: full weighting
-// at the node itself plus, for nodes next to a Neumann/Robin face, the full
-// weighting at every boundary node whose closure chain ends here, times the
-// chain's coefficient. The transpose of the extended prolongation below, so
-// the V-cycle stays a symmetric preconditioner. Each coarse node gathers its
-// own value: race free.
+// Restriction R = Ext^T P^T / 2^dim, in two race-free launches:
+//  k_restrict_fw   full weighting of the fine residual at every coarse node,
+//                  boundary nodes included (one thread per coarse node);
+//  k_restrict_fold interior coarse nodes next to a Neumann/Robin face add
+//                  coef * value of each boundary node whose closure chain ends
+//                  at them (the transpose of the extended prolongation below).
+// Boundary entries of the coarse right-hand side are left holding their full
+// weights; no coarse kernel reads them.
 template <typename T, typename TC>
-__global__ void __launch_bounds__(kBx* kBy) k_restrict(GridDev gf, GridDev gc, const T* __restrict__ rf,
-                                                       TC* __restrict__ bc, const Ctl* ctl) {
+__global__ void __launch_bounds__(kBx* kBy) k_restrict_fw(GridDev gf, GridDev gc, const T* __restrict__ rf,
+                                                          TC* __restrict__ bc, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int I = blockIdx.x * kBx + threadIdx.x;
+  const int J = blockIdx.y * kBy + threadIdx.y;
+  if (I >= gc.nx || J >= gc.ny) return;
+  const int chunk = (gc.nz + gridDim.z - 1) / gridDim.z;
+  const int K0 = blockIdx.z * chunk, K1 = min(gc.nz, K0 + chunk);
+  for (int K = K0; K < K1; ++K) bc[cidx(gc, I, J, K)] = TC(full_weight<T>(gf, gc, rf, I, J, K));
+}
+
+template <typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_restrict_fold(GridDev gc, TC* __restrict__ bc, const Ctl* ctl) {
   if (ctl_skip(ctl)) return;
   const int I = blockIdx.x * kBx + threadIdx.x;
   const int J = blockIdx.y * kBy + threadIdx.y;
@@ -502,24 +663,21 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict(GridDev gf, GridDev gc, c
   const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
   for (int K = K0; K < K1; ++K) {
     const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+    if (dxl == 0 && dxh == 0 && dyl == 0 && dyh == 0 && dzl == 0 && dzh == 0) continue;
     double acc = 0.0;
     for (int dk = dzl; dk <= dzh; ++dk)
       for (int dj = dyl; dj <= dyh; ++dj)
         for (int di = dxl; di <= dxh; ++di) {
-          if (di == 0 && dj == 0 && dk == 0) {
-            acc += full_weight<T>(gf, gc, rf, I, J, K);
-            continue;
-          }
+          if (di == 0 && dj == 0 && dk == 0) continue;
           int ci = I + di, cj = J + dj, ck = K + dk;
           const double coef = ext_chain(gc, ci, cj, ck);
-          if (coef != 0.0 && ci == I && cj == J && ck == K) acc += coef * full_weight<T>(gf, gc, rf, I + di, J + dj, K + dk);
+          if (coef != 0.0 && ci == I && cj == J && ck == K) acc += coef * double(bc[cidx(gc, I + di, J + dj, K + dk)]);
         }
-    bc[((long long)K * gc.ny + J) * gc.nx + I] = TC(acc);
+    if (acc != 0.0) {
+      const long long id = cidx(gc, I, J, K);
+      bc[id] = TC(double(bc[id]) + acc);
+    }
   }
-}
-
-__device__ __forceinline__ long long cidx(const GridDev& g, int i, int j, int k) {
-  return ((long long)k * g.ny + j) * g.nx + i;
 }
 
 // coarse correction value at any coarse node, boundary nodes by the
@@ -601,6 +759,59 @@ __global__ void k_coarse_solve(GridDev g, Coef cf, const TB* __restrict__ b, T* 
       __syncthreads();
     }
   }
+}
+
+// Coarsest level in shared memory: the folded stencils of all interior nodes
+// are evaluated once, then `sweeps` red-black sweeps run on-chip from zero.
+// For coarsest grids of at most kCoarseMaxNodes nodes / kCoarseMaxInterior
+// interior nodes (checked by the host).
+constexpr int kCoarseMaxNodes = 1024;
+constexpr int kCoarseMaxInterior = 512;
+
+template <class Coef, typename T, typename TB>
+__global__ void k_coarse_solve_smem(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x, int sweeps,
+                                    const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  __shared__ T sx[kCoarseMaxNodes];
+  __shared__ T sb[kCoarseMaxInterior];
+  __shared__ T sw[kCoarseMaxInterior][7];
+  __shared__ int sid[kCoarseMaxInterior];
+  const int tid = threadIdx.x;
+  const int n = (int)g.n;
+  for (int t = tid; t < n; t += blockDim.x) sx[t] = T(0);
+  const int kb = g.dim == 3 ? 1 : 0, ke = g.dim == 3 ? g.nz - 1 : 1;
+  const int ni = g.nx - 2, nj = g.ny - 2, nk = ke - kb;
+  const int total = ni * nj * nk;
+  for (int t = tid; t < total; t += blockDim.x) {
+    const int i = 1 + t % ni, j = 1 + (t / ni) % nj, k = kb + t / (ni * nj);
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    Stencil<T> st = cf.template at<T>(g, id);
+    fold_faces<T>(g, i, j, k, st, nullptr);
+    sw[t][0] = st.c;
+    sw[t][1] = st.xp;
+    sw[t][2] = st.xm;
+    sw[t][3] = st.yp;
+    sw[t][4] = st.ym;
+    sw[t][5] = st.zp;
+    sw[t][6] = st.zm;
+    sb[t] = T(b[id]);
+    sid[t] = (int)id;
+  }
+  __syncthreads();
+  const int sxy = (int)g.sxy, nx = g.nx;
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      for (int t = tid; t < total; t += blockDim.x) {
+        const int i = 1 + t % ni, j = 1 + (t / ni) % nj, k = kb + t / (ni * nj);
+        if (((i + j + k) & 1) != color) continue;
+        const int id = sid[t];
+        T v = sw[t][1] * sx[id + 1] + sw[t][2] * sx[id - 1] + sw[t][3] * sx[id + nx] + sw[t][4] * sx[id - nx];
+        if (g.dim == 3) v = v + sw[t][5] * sx[id + sxy] + sw[t][6] * sx[id - sxy];
+        sx[id] = (sb[t] - v) / sw[t][0];
+      }
+      __syncthreads();
+    }
+  for (int t = tid; t < n; t += blockDim.x) x[t] = sx[t];
 }
 
 }  // namespace pdeb

@@ -1,0 +1,488 @@
+// Device residual norms, explicit time stepping and pressure projection.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "host.h"
+#include "solvers.cuh"
+
+namespace pdeb {
+
+// ------------------------------------------------------------ residual norms
+
+struct PostAux {
+  Ctl* c;
+  int slot;
+  __device__ void operator()(const double* v) const { c->aux[slot] = v[0]; }
+};
+
+// ComputeResidualNorms (src/residual.cpp:153-723): 2D visits every node and
+// boundary nodes use their closure with alpha + beta/h on every Robin face
+// (:359,399); interior r = center*u + neighbours + f. 3D is interior only.
+template <class Coef>
+__global__ void k_residual_norms(GridDev g, Coef cf, const double* __restrict__ f, double fc,
+                                 const double* __restrict__ u, RedSlot s_sum, RedSlot s_max, Ctl* out) {
+  double acc[1] = {0.0}, mx[1] = {0.0};
+  for (long long t = gtid(); t < g.n; t += gstride()) {
+    const int i = int(t % g.nx), j = int((t / g.nx) % g.ny), k = int(t / g.sxy);
+    const bool bd = i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || (g.dim == 3 && (k == 0 || k == g.nz - 1));
+    double r;
+    if (bd) {
+      if (g.dim == 3) continue;
+      int face, nbi = i, nbj = j;
+      if (i == 0) { face = kLeft; nbi = 1; }
+      else if (i == g.nx - 1) { face = kRight; nbi = g.nx - 2; }
+      else if (j == 0) { face = kBottom; nbj = 1; }
+      else { face = kTop; nbj = g.ny - 2; }
+      const FaceDev& F = g.face[face];
+      const int loc = face_loc(g, face, i, j, k);
+      const double un = u[(long long)nbj * g.nx + nbi];
+      if (F.kind == kDirichlet) {
+        r = u[t] - F.val.at(loc);
+      } else if (F.kind == kNeumann) {
+        const double gv = F.val.at(loc);
+        r = u[t] - ((face & 1) ? un + F.h * gv : un - F.h * gv);
+      } else {
+        const double alpha = F.alpha.at(loc), beta = F.beta.at(loc), gamma = F.gamma.at(loc);
+        const double denom = alpha + beta / F.h;
+        if (!(fabs(denom) > 1e-12)) continue;
+        r = u[t] - (gamma + (beta / F.h) * un) / denom;
+      }
+    } else {
+      const Stencil<double> s = cf.template at<double>(g, t);
+      const double zp = g.dim == 3 ? u[t + g.sxy] : 0.0, zm = g.dim == 3 ? u[t - g.sxy] : 0.0;
+      r = s.c * u[t] + nb_sum<double>(s, u[t + 1], u[t - 1], u[t + g.nx], u[t - g.nx], zp, zm, g.dim) +
+          (f ? f[t] : fc);
+    }
+    acc[0] += r * r;
+    mx[0] = fmax(mx[0], fabs(r));
+  }
+  grid_reduce<1, false>(acc, s_sum, PostAux{out, 0});
+  grid_reduce<1, true>(mx, s_max, PostAux{out, 1});
+}
+
+pdeb200_status residual_norms_dev(Context* ctx, DevProblem& P, const double* d_grid, double* l2, double* linf) {
+  with_coef(P, [&](const auto& cf) {
+    using Coef = std::decay_t<decltype(cf)>;
+    k_residual_norms<Coef><<<vec_blocks(P.g.n, ctx), 256, 0, ctx->stream>>>(P.g, cf, P.f, P.f_const, d_grid,
+                                                                            ctx->slot(0), ctx->slot(1), ctx->d_ctl);
+  });
+  ctx->count();
+  const Ctl& c = ctl_poll(ctx);
+  *l2 = std::sqrt(c.aux[0] > 0 ? c.aux[0] : 0.0);
+  *linf = c.aux[1];
+  return PDEB200_OK;
+}
+
+// -------------------------------------------------------------- time series
+
+// One forward-Euler step of SolvePDETimeSeries (solver.cpp:1282-1319):
+// interior next = u + dt * SafeDivClamped(-(L u + f), ut, 0); boundary nodes
+// copied (their closures at t+dt follow in k_fill_boundary).
+template <class Coef>
+__global__ void __launch_bounds__(kBx* kBy) k_fe_step(GridDev g, Coef cf, const double* __restrict__ f, double fc,
+                                                      double ut, double dt, const double* __restrict__ u,
+                                                      double* __restrict__ next) {
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int chunk = (g.nz + gridDim.z - 1) / gridDim.z;
+  const int k0 = blockIdx.z * chunk, k1 = min(g.nz, k0 + chunk);
+  for (int k = k0; k < k1; ++k) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    const bool interior = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && (g.dim == 2 || (k >= 1 && k <= g.nz - 2));
+    if (!interior) {
+      next[id] = u[id];
+      continue;
+    }
+    const Stencil<double> s = cf.template at<double>(g, id);
+    const double zp = g.dim == 3 ? u[id + g.sxy] : 0.0, zm = g.dim == 3 ? u[id - g.sxy] : 0.0;
+    const double opv = s.c * u[id] + nb_sum<double>(s, u[id + 1], u[id - 1], u[id + g.nx], u[id - g.nx], zp, zm, g.dim);
+    const double rhs = opv + (f ? f[id] : fc);
+    double u_t = 0.0;
+    if (!(fabs(ut) < 1e-12)) {
+      u_t = -rhs / ut;
+      if (!isfinite(u_t)) u_t = 0.0;
+    }
+    next[id] = u[id] + dt * u_t;
+  }
+}
+
+pdeb200_status time_series_dev(Context* ctx, DevProblem& P, const pdeb200_time_options* t, pdeb200_frame_cb cb,
+                               void* user, bool host_frames, double* d_out, pdeb200_report* rep) {
+  if (!(t->dt > 0.0)) throw StatusFailure{PDEB200_ERR_INVALID, "time step dt must be positive"};
+  const GridDev& g = P.g;
+  const long long n = g.n;
+  const int frames = t->frames > 1 ? t->frames : 1;
+  const int stride = t->frame_stride > 0 ? t->frame_stride : 1;
+  Buf other(sizeof(double) * n, ctx->stream);
+  double* buf[2] = {d_out, other.as<double>()};
+  if (P.u0)
+    PDEB_CUDA(cudaMemcpyAsync(buf[0], P.u0, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+  else
+    PDEB_CUDA(cudaMemsetAsync(buf[0], 0, sizeof(double) * n, ctx->stream));
+  fill_boundary(ctx, g, buf[0], nullptr);
+  std::vector<double> host;
+  double* pinned = nullptr;
+  if (cb && host_frames) PDEB_CUDA(cudaMallocHost(&pinned, sizeof(double) * n));
+  int cur = 0;
+  pdeb200_status st = PDEB200_OK;
+  PDEB_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  const dim3 grid = stencil_grid_full(g), block = stencil_block();
+  for (int frame = 0; frame < frames; ++frame) {
+    if (cb && (frame % stride == 0 || frame + 1 == frames)) {
+      const double time = t->t_start + frame * t->dt;
+      const double* view = buf[cur];
+      if (host_frames) {
+        PDEB_CUDA(cudaMemcpyAsync(pinned, buf[cur], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+        view = pinned;
+      } else {
+        PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+      }
+      if (!cb(frame, time, view, user)) break;
+    }
+    if (frame + 1 >= frames) break;
+    with_coef(P, [&](const auto& cf) {
+      using Coef = std::decay_t<decltype(cf)>;
+      k_fe_step<Coef><<<grid, block, 0, ctx->stream>>>(g, cf, P.f, P.f_const, P.ut, t->dt, buf[cur], buf[cur ^ 1]);
+    });
+    ctx->count();
+    cur ^= 1;
+    fill_boundary(ctx, g, buf[cur], nullptr);
+    if (rep) rep->iterations = frame + 1;
+  }
+  PDEB_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (cur == 1) PDEB_CUDA(cudaMemcpyAsync(d_out, buf[1], sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (rep) {
+    rep->device_ms = ms;
+    rep->converged = 1;
+  }
+  if (pinned) cudaFreeHost(pinned);
+  return st;
+}
+
+// ---------------------------------------------------------------- projection
+
+struct ProjGrid {
+  int nx, ny, nz, is3;
+  long long n, sxy;
+  double dx, dy, dz;
+};
+
+// Collocated divergence, central inside and one-sided at walls
+// (pressure_projection.cpp:11-46, 471-520); optional sums of div^2 and max|div|.
+__global__ void k_divergence(ProjGrid g, const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ w, double* __restrict__ div, double dt,
+                             double* __restrict__ rhs, RedSlot s_sum, RedSlot s_max, Ctl* out, int aux0) {
+  double acc[1] = {0.0}, mx[1] = {0.0};
+  for (long long t = gtid(); t < g.n; t += gstride()) {
+    const int i = int(t % g.nx), j = int((t / g.nx) % g.ny), k = int(t / g.sxy);
+    double du, dv, dw = 0.0;
+    if (i == 0) du = (u[t + 1] - u[t]) / g.dx;
+    else if (i == g.nx - 1) du = (u[t] - u[t - 1]) / g.dx;
+    else du = (u[t + 1] - u[t - 1]) / (2.0 * g.dx);
+    if (j == 0) dv = (v[t + g.nx] - v[t]) / g.dy;
+    else if (j == g.ny - 1) dv = (v[t] - v[t - g.nx]) / g.dy;
+    else dv = (v[t + g.nx] - v[t - g.nx]) / (2.0 * g.dy);
+    double d;
+    if (g.is3) {
+      if (k == 0) dw = (w[t + g.sxy] - w[t]) / g.dz;
+      else if (k == g.nz - 1) dw = (w[t] - w[t - g.sxy]) / g.dz;
+      else dw = (w[t + g.sxy] - w[t - g.sxy]) / (2.0 * g.dz);
+      d = du + dv + dw;
+    } else {
+      d = du + dv;
+    }
+    div[t] = d;
+    if (rhs) rhs[t] = d / dt;
+    acc[0] += d * d;
+    mx[0] = fmax(mx[0], fabs(d));
+  }
+  grid_reduce<1, false>(acc, s_sum, PostAux{out, aux0});
+  grid_reduce<1, true>(mx, s_max, PostAux{out, aux0 + 1});
+}
+
+// Neumann (copy-ghost) Laplacian: 2D cx(xp-2xc+xm)+cy(..) (:136-151), 3D
+// cc*xc + cx*xm + ... with p[0] pinned when requested (:530-560); fused sum(Ap)
+// (2D mean projection) or sum(p*Ap) (3D).
+template <class Post>
+__global__ void k_proj_laplace(ProjGrid g, const double* __restrict__ x, double* __restrict__ y, int pin,
+                               int dot_with_x, RedSlot slot, Post post, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const double cx = 1.0 / (g.dx * g.dx), cy = 1.0 / (g.dy * g.dy), cz = g.is3 ? 1.0 / (g.dz * g.dz) : 0.0;
+  const double cc = -2.0 * (cx + cy + cz);
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < g.n; t += gstride()) {
+    const int i = int(t % g.nx), j = int((t / g.nx) % g.ny), k = int(t / g.sxy);
+    const double xc = x[t];
+    double val;
+    if (!g.is3) {
+      const double xm = i > 0 ? x[t - 1] : xc, xp = i < g.nx - 1 ? x[t + 1] : xc;
+      const double ym = j > 0 ? x[t - g.nx] : xc, yp = j < g.ny - 1 ? x[t + g.nx] : xc;
+      val = cx * (xp - 2.0 * xc + xm) + cy * (yp - 2.0 * xc + ym);
+    } else {
+      double lap = cc * xc;
+      lap += cx * (i > 0 ? x[t - 1] : xc);
+      lap += cx * (i < g.nx - 1 ? x[t + 1] : xc);
+      lap += cy * (j > 0 ? x[t - g.nx] : xc);
+      lap += cy * (j < g.ny - 1 ? x[t + g.nx] : xc);
+      lap += cz * (k > 0 ? x[t - g.sxy] : xc);
+      lap += cz * (k < g.nz - 1 ? x[t + g.sxy] : xc);
+      val = lap;
+      if (pin && t == 0) val = xc;
+    }
+    y[t] = val;
+    acc[0] += dot_with_x ? xc * val : val;
+  }
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+// y -= mean (mean = sum/n read from src->aux[q]); optional sum(w*y).
+// `skip` (may be null) is the control block whose done flag ends the kernel.
+template <class Post>
+__global__ void k_sub_mean(long long n, double* __restrict__ y, const double* __restrict__ w, int q, RedSlot slot,
+                           Post post, const Ctl* src, const Ctl* skip) {
+  if (ctl_skip(skip)) return;
+  const double mean = src->aux[q] / double(n);
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < n; t += gstride()) {
+    const double v = y[t] - mean;
+    y[t] = v;
+    if (w) acc[0] += w[t] * v;
+  }
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+__global__ void k_sum(long long n, const double* __restrict__ a, RedSlot slot, PostAux post) {
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < n; t += gstride()) acc[0] += a[t];
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+// pure-Neumann CG posts (pressure_projection.cpp:160-230)
+struct PostProjAlpha {
+  Ctl* c;
+  int is3;
+  __device__ void operator()(const double* v) const {
+    if (fabs(v[0]) < 1e-30) {
+      c->done = 1;
+      c->status = is3 ? PDEB200_ERR_BREAKDOWN : PDEB200_OK;  // 2D returns success here, 3D failure
+      c->aux[7] = 1.0;                                        // breakdown flag: no mean removal
+      return;
+    }
+    c->alpha = c->rr / v[0];
+  }
+};
+
+struct PostProjRR {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->iter += 1;
+    const double rn = sqrt(v[0]);
+    if (rn < c->tol * c->aux[6] || rn < 1e-14) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+      c->aux[5] = rn;
+      return;
+    }
+    c->beta = v[0] / c->rr;
+    c->rr = v[0];
+    if (c->iter >= c->max_iter) {
+      c->done = 1;
+      c->status = PDEB200_ERR_NOT_CONVERGED;
+      c->aux[5] = sqrt(c->rr);
+    }
+  }
+};
+
+struct PostProjR0 {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    c->rr = v[0];
+    c->aux[6] = sqrt(v[0]);
+    if (sqrt(v[0]) < 1e-15) {
+      c->done = 1;
+      c->status = PDEB200_OK;
+      c->aux[5] = 0.0;
+      c->aux[4] = 1.0;  // zero initial residual: no update of p at all
+    }
+  }
+};
+
+__global__ void k_proj_xr(long long n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                          const double* __restrict__ q, RedSlot slot, PostProjRR post, Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const double a = ctl->alpha;
+  double acc[1] = {0.0};
+  for (long long t = gtid(); t < n; t += gstride()) {
+    x[t] += a * p[t];
+    const double rv = r[t] - a * q[t];
+    r[t] = rv;
+    acc[0] += rv * rv;
+  }
+  grid_reduce<1, false>(acc, slot, post);
+}
+
+// u -= dt * grad p (central inside, one-sided at walls; :75-104, 563-605)
+__global__ void k_grad_update(ProjGrid g, const double* __restrict__ p, double* __restrict__ u, double* __restrict__ v,
+                              double* __restrict__ w, double dt) {
+  for (long long t = gtid(); t < g.n; t += gstride()) {
+    const int i = int(t % g.nx), j = int((t / g.nx) % g.ny), k = int(t / g.sxy);
+    double gx, gy;
+    if (i == 0) gx = (p[t + 1] - p[t]) / g.dx;
+    else if (i == g.nx - 1) gx = (p[t] - p[t - 1]) / g.dx;
+    else gx = (p[t + 1] - p[t - 1]) / (2.0 * g.dx);
+    if (j == 0) gy = (p[t + g.nx] - p[t]) / g.dy;
+    else if (j == g.ny - 1) gy = (p[t] - p[t - g.nx]) / g.dy;
+    else gy = (p[t + g.nx] - p[t - g.nx]) / (2.0 * g.dy);
+    u[t] -= dt * gx;
+    v[t] -= dt * gy;
+    if (g.is3) {
+      double gz;
+      if (k == 0) gz = (p[t + g.sxy] - p[t]) / g.dz;
+      else if (k == g.nz - 1) gz = (p[t] - p[t - g.sxy]) / g.dz;
+      else gz = (p[t + g.sxy] - p[t - g.sxy]) / (2.0 * g.dz);
+      w[t] -= dt * gz;
+    }
+  }
+}
+
+__global__ void k_axpy_set(long long n, double* __restrict__ y, const double* __restrict__ a,
+                           const double* __restrict__ b) {
+  for (long long t = gtid(); t < n; t += gstride()) y[t] = a[t] - b[t];
+}
+
+struct PostStoreRROnly {
+  Ctl* c;
+  __device__ void operator()(const double* v) const { c->rr = v[0]; }
+};
+
+pdeb200_status project_dev(Context* ctx, int nx, int ny, int nz, double dx, double dy, double dz, double dt,
+                           double* u, double* v, double* w, double* p, const pdeb200_projection_options* po,
+                           pdeb200_projection_report* rep) {
+  ProjGrid g{nx, ny, nz > 1 ? nz : 1, nz > 1 ? 1 : 0, 0, 0, dx, dy, dz};
+  g.sxy = (long long)nx * ny;
+  g.n = g.sxy * g.nz;
+  const long long n = g.n;
+  const bool host = po->mem_space != PDEB200_MEM_DEVICE;
+  const int nfields = g.is3 ? 4 : 3;
+  std::vector<Buf> fb;
+  double* d[4] = {u, v, w, p};
+  double* host_ptr[4] = {u, v, w, p};
+  if (host) {
+    for (int q = 0; q < 4; ++q) {
+      if (q == 2 && !g.is3) {
+        d[q] = nullptr;
+        continue;
+      }
+      fb.emplace_back(sizeof(double) * n, ctx->stream);
+      d[q] = fb.back().as<double>();
+      PDEB_CUDA(cudaMemcpyAsync(d[q], host_ptr[q], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    }
+  }
+  (void)nfields;
+  double *du = d[0], *dv = d[1], *dw = d[2], *dp = d[3];
+  Buf divb(sizeof(double) * n, ctx->stream), rhsb(sizeof(double) * n, ctx->stream), rb(sizeof(double) * n, ctx->stream),
+      pcb(sizeof(double) * n, ctx->stream), apb(sizeof(double) * n, ctx->stream);
+  double *div = divb.as<double>(), *rhs = rhsb.as<double>(), *r = rb.as<double>(), *pc = pcb.as<double>(),
+         *ap = apb.as<double>();
+  const int nb = vec_blocks(n, ctx);
+  PDEB_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ctl_init(ctx, po->max_iter, po->tol, 1e-30);
+  Ctl* C = ctx->d_ctl;
+  // divergence before, rhs = div/dt
+  k_divergence<<<nb, 256, 0, ctx->stream>>>(g, du, dv, dw, div, dt, rhs, ctx->slot(0), ctx->slot(1), C, 0);
+  // rhs -= mean(rhs); 3D pins rhs[0]
+  k_sum<<<nb, 256, 0, ctx->stream>>>(n, rhs, ctx->slot(0), PostAux{C, 2});
+  k_sub_mean<NoPost><<<nb, 256, 0, ctx->stream>>>(n, rhs, nullptr, 2, ctx->slot(0), NoPost{}, C, nullptr);
+  const int pin = g.is3 && po->fix_pressure_corner;
+  if (pin) PDEB_CUDA(cudaMemcpyAsync(rhs, &po->reference_pressure, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  // r = rhs - A p, (2D) r -= mean(r), pc = r, rr
+  k_proj_laplace<NoPost><<<nb, 256, 0, ctx->stream>>>(g, dp, ap, pin, 0, ctx->slot(0), NoPost{}, nullptr);
+  k_axpy_set<<<nb, 256, 0, ctx->stream>>>(n, r, rhs, ap);
+  if (!g.is3) {
+    k_sum<<<nb, 256, 0, ctx->stream>>>(n, r, ctx->slot(0), PostAux{C, 3});
+    k_sub_mean<NoPost><<<nb, 256, 0, ctx->stream>>>(n, r, nullptr, 3, ctx->slot(0), NoPost{}, C, nullptr);
+  }
+  PDEB_CUDA(cudaMemcpyAsync(pc, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+  k_dot<double, PostProjR0><<<nb, 256, 0, ctx->stream>>>(n, r, r, ctx->slot(0), PostProjR0{C}, nullptr);
+  ctx->count(8);
+  auto iterate = [&](int) {
+    if (!g.is3) {
+      // Ap = L p, sum(Ap) -> mean; Ap -= mean with p.Ap -> alpha
+      k_proj_laplace<PostAux><<<nb, 256, 0, ctx->stream>>>(g, pc, ap, 0, 0, ctx->slot(0), PostAux{C, 3}, C);
+      k_sub_mean<PostProjAlpha><<<nb, 256, 0, ctx->stream>>>(n, ap, pc, 3, ctx->slot(0), PostProjAlpha{C, 0}, C, C);
+      ctx->count(2);
+    } else {
+      k_proj_laplace<PostProjAlpha><<<nb, 256, 0, ctx->stream>>>(g, pc, ap, pin, 1, ctx->slot(0),
+                                                                 PostProjAlpha{C, 1}, C);
+      ctx->count();
+    }
+    k_proj_xr<<<nb, 256, 0, ctx->stream>>>(n, dp, r, pc, ap, ctx->slot(0), PostProjRR{C}, C);
+    k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, pc, r, C, 0);
+    ctx->count(2);
+  };
+  pdeb200_options o{};
+  o.check_interval = 32;
+  pdeb200_status st = drive(ctx, &o, po->max_iter + 1, iterate, false);
+  const Ctl c = ctl_poll(ctx);
+  const bool zero_start = c.aux[4] != 0.0;
+  const bool breakdown = c.aux[7] != 0.0;
+  bool ok;
+  int iters = c.iter;
+  if (zero_start) {
+    ok = true;
+    iters = 0;
+  } else if (breakdown) {
+    ok = !g.is3;  // 2D: converged (no mean removal); 3D: failure
+  } else if (c.done && c.status == PDEB200_OK) {
+    ok = true;
+  } else {
+    ok = !g.is3;  // max_iter: 2D keeps the approximation
+    iters = po->max_iter;
+  }
+  const bool remove_mean = ok && !zero_start && !breakdown;
+  if (remove_mean) {
+    k_sum<<<nb, 256, 0, ctx->stream>>>(n, dp, ctx->slot(0), PostAux{C, 2});
+    k_sub_mean<NoPost><<<nb, 256, 0, ctx->stream>>>(n, dp, nullptr, 2, ctx->slot(0), NoPost{}, C, nullptr);
+    ctx->count(2);
+  }
+  if (rep) {
+    rep->poisson_iterations = iters;
+    rep->poisson_residual = zero_start ? 0.0
+                            : (c.done && c.status == PDEB200_OK && !breakdown) ? c.aux[5]
+                                                                               : std::sqrt(c.rr);
+    rep->l2_divergence_before = std::sqrt(c.aux[0] / n);
+    rep->max_divergence_before = c.aux[1];
+  }
+  if (ok) {
+    k_grad_update<<<nb, 256, 0, ctx->stream>>>(g, dp, du, dv, dw, dt);
+    k_divergence<<<nb, 256, 0, ctx->stream>>>(g, du, dv, dw, div, 1.0, nullptr, ctx->slot(0), ctx->slot(1), C, 0);
+    ctx->count(2);
+    const Ctl& c2 = ctl_poll(ctx);
+    if (rep) {
+      rep->l2_divergence_after = std::sqrt(c2.aux[0] / n);
+      rep->max_divergence_after = c2.aux[1];
+    }
+  }
+  PDEB_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (host) {
+    for (int q = 0; q < 4; ++q)
+      if (d[q]) PDEB_CUDA(cudaMemcpyAsync(host_ptr[q], d[q], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (rep) {
+    rep->device_ms = ms;
+    rep->success = ok ? 1 : 0;
+  }
+  (void)st;
+  return ok ? PDEB200_OK : PDEB200_ERR_NOT_CONVERGED;
+}
+
+}  // namespace pdeb

@@ -93,6 +93,30 @@ dim3 stencil_grid(const GridDev& g, int zchunk) {
   return dim3(xy.x, xy.y, cap_chunks((long long)xy.x * xy.y, chunks));
 }
 
+dim3 stencil_grid_auto(const GridDev& g) {
+  const long long kTargetBlocks = 148 * 16;
+  const int kint = g.dim == 3 ? g.nz - 2 : 1;
+  const dim3 xy((g.nx + kBx - 1) / kBx, (g.ny + kBy - 1) / kBy, 1);
+  const long long xyb = (long long)xy.x * xy.y;
+  long long chunks = (kTargetBlocks + xyb - 1) / xyb;
+  if (chunks > kint) chunks = kint;
+  if (chunks < 1) chunks = 1;
+  return dim3(xy.x, xy.y, cap_chunks(xyb, (int)chunks));
+}
+
+dim3 fused_grid(const GridDev& g) {
+  const long long kTargetBlocks = 148 * 8;
+  const int kint = g.dim == 3 ? g.nz - 2 : 1;
+  const dim3 xy((g.nx + kFx - 1) / kFx, (g.ny + kBy - 1) / kBy, 1);
+  const long long xyb = (long long)xy.x * xy.y;
+  long long chunks = (kTargetBlocks + xyb - 1) / xyb;
+  // at least two slabs per chunk so the halo planes are amortised
+  const long long max_chunks = (kint + 2 * kSlab - 1) / (2 * kSlab);
+  if (chunks > max_chunks) chunks = max_chunks;
+  if (chunks < 1) chunks = 1;
+  return dim3(xy.x, xy.y, cap_chunks(xyb, (int)chunks));
+}
+
 dim3 stencil_grid_full(const GridDev& g, int zchunk) {
   const int chunks = (g.nz + zchunk - 1) / zchunk;
   const dim3 xy((g.nx + kBx - 1) / kBx, (g.ny + kBy - 1) / kBy, 1);

@@ -134,33 +134,33 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
   k_dot<double, PostBB><<<nb, 256, 0, ctx->stream>>>(n, bf, bf, ctx->slot(), PostBB{ctx->d_ctl}, ctx->d_ctl);
   ctx->count();
   (void)b;
-  // z = M r (z lives in level-0 x), p = z, rz = r.z
-  double* z = H.levels[0].x;
+  // z = M r (z is the level-0 result buffer), p = z, rz = r.z
+  double* z = H.z();
   H.vcycle(ctx, r, ctx->d_ctl);
   k_dot<double, PostRZ><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostRZ{ctx->d_ctl}, ctx->d_ctl);
   k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 1);
   ctx->count(2);
-  const dim3 grid = stencil_grid(g), block = stencil_block();
+  const dim3 grid = stencil_grid_auto(g), block = stencil_block();
   const double dofs = interior_dofs(g);
   auto iterate = [&](int) {
     {
-      ProfScope ps(ctx, "apply_dot", dofs * 24.0, true);
+      ProfScope ps(ctx, "apply_dot", 0, dofs * 24.0);
       k_apply_folded<Coef, double, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(),
                                                                                    PostAlpha{ctx->d_ctl}, ctx->d_ctl);
     }
     {
-      ProfScope ps(ctx, "cg_update_xr", dofs * 48.0, true);
+      ProfScope ps(ctx, "cg_update_xr", 0, dofs * 48.0);
       k_cg_xr<double, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, d_x, r, p, q, ctx->slot(), PostRRRel{ctx->d_ctl},
                                                               ctx->d_ctl);
     }
     ctx->count(2);
     H.vcycle(ctx, r, ctx->d_ctl);
     {
-      ProfScope ps(ctx, "dot", dofs * 16.0, true);
+      ProfScope ps(ctx, "dot", 0, dofs * 16.0);
       k_dot<double, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{ctx->d_ctl}, ctx->d_ctl);
     }
     {
-      ProfScope ps(ctx, "cg_update_p", dofs * 24.0, true);
+      ProfScope ps(ctx, "cg_update_p", 0, dofs * 24.0);
       k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 0);
     }
     ctx->count(2);

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -176,10 +177,10 @@ pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& 
   }
 }
 
-inline void fill_boundary(Context* ctx, const GridDev& g, double* u, const Ctl* ctl) {
+inline void fill_boundary(Context* ctx, const GridDev& g, double* u, const Ctl* ctl, bool dirichlet_last = true) {
   const long long faces = 2LL * g.ny * g.nz + 2LL * g.nx * g.nz + (g.dim == 3 ? 2LL * g.nx * g.ny : 0);
   const int blocks = vec_blocks(faces, ctx);
-  k_fill_boundary<<<blocks, 256, 0, ctx->stream>>>(g, u, ctl);
+  k_fill_boundary<<<blocks, 256, 0, ctx->stream>>>(g, u, ctl, dirichlet_last ? 1 : 0);
   ctx->count();
 }
 
@@ -285,9 +286,18 @@ inline void inject_k(Context* ctx, const GridDev& gf, const GridDev& gc, const K
 
 // Coarse coefficients: constants are re-evaluated with the coarse spacing,
 // sampled fields are injected (k_c(I) = k_f(2I)).
+// Coarse constant stencils are rediscretised at the coarse spacing. With
+// convection, the coarse diffusion is raised where needed so the coarse cell
+// Peclet number |c| H / (2|a|) stays <= 1 (central differences keep a
+// diagonally dominant coarse operator); the fine operator is never modified.
 inline CoefConst coarsen_coef(Context*, const DevProblem& P, const CoefConst&, const GridDev&, const GridDev& gc,
                               double dx, double dy, double dz, std::vector<Buf>*) {
-  return make_const(P.a, P.b, P.az, P.c, P.d, P.dzc, P.e, dx, dy, dz, gc.dim);
+  auto stab = [](double a, double c, double h) {
+    const double need = std::fabs(c) * h * 0.5;
+    return (a <= 0.0 && -a < need) ? -need : a;
+  };
+  return make_const(stab(P.a, P.c, dx), stab(P.b, P.d, dy), gc.dim == 3 ? stab(P.az, P.dzc, dz) : P.az, P.c, P.d,
+                    P.dzc, P.e, dx, dy, dz, gc.dim);
 }
 
 template <typename KT>
@@ -325,21 +335,25 @@ inline CoefNodal coarsen_coef(Context* ctx, const DevProblem&, const CoefNodal& 
 }
 
 // Geometric hierarchy of the folded operator. Coarsening n_c = (n+1)/2 while
-// every active dimension is odd and >= 5, stopping once a dimension reaches 5
-// or mg_max_levels (the rule of multigrid.cpp:150-170); face closures are
-// rediscretised with the coarse spacing. Vectors of type T.
+// every active dimension is odd and >= 5 (down to 3 nodes in the smallest
+// dimension); face closures are rediscretised with the coarse spacing.
+// Each level has two field buffers: smoothing sweeps are fused red-black
+// passes that read one buffer and write the other.
 template <class Coef, typename T>
 struct Hierarchy {
   struct Level {
     GridDev g;
     Coef cf;
-    T* x;
+    T* xa;   // written by the first sweep from zero
+    T* xb;
     T* b;
     T* r;
+    T* out;  // buffer holding this level's result after a V-cycle
   };
   std::vector<Level> levels;
   std::vector<Buf> owned;
   int pre = 2, post = 2, coarse_iters = 50;
+  bool needs_fold = false;  // some face is Neumann/Robin
 
   T* alloc(Context* ctx, long long n) {
     owned.emplace_back(sizeof(T) * n, ctx->stream);
@@ -348,7 +362,16 @@ struct Hierarchy {
     return p;
   }
 
+  bool coarse_in_smem(const Level& L) const {
+    const long long interior = (long long)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.dim == 3 ? L.g.nz - 2 : 1);
+    return L.g.n <= kCoarseMaxNodes && interior <= kCoarseMaxInterior;
+  }
+
   void build(Context* ctx, DevProblem& P, const pdeb200_problem* hp, const Coef& cf0, const pdeb200_options* o) {
+    fused = std::getenv("PDEB200_FUSED_SWEEP") != nullptr;
+    needs_fold = false;
+    for (int f = 0; f < 6; ++f)
+      if (P.g.face[f].active && P.g.face[f].kind != kDirichlet) needs_fold = true;
     pre = o->mg_pre_smooth > 0 ? o->mg_pre_smooth : 0;
     post = o->mg_post_smooth > 0 ? o->mg_post_smooth : 0;
     coarse_iters = o->mg_coarse_iters > 1 ? o->mg_coarse_iters : 1;
@@ -356,11 +379,11 @@ struct Hierarchy {
     Level l0;
     l0.g = P.g;
     l0.cf = cf0;
-    l0.x = alloc(ctx, P.g.n);
+    l0.xa = alloc(ctx, P.g.n);
+    l0.xb = alloc(ctx, P.g.n);
     l0.b = nullptr;
     l0.r = alloc(ctx, P.g.n);
     levels.push_back(l0);
-    double dx = P.dx, dy = P.dy, dz = P.dz;
     int stride = 1;
     while ((int)levels.size() < max_levels && can_coarsen(levels.back().g)) {
       const GridDev& gf = levels.back().g;
@@ -371,79 +394,124 @@ struct Hierarchy {
       c.g.nz = gf.dim == 3 ? (gf.nz + 1) / 2 : 1;
       c.g.sxy = (long long)c.g.nx * c.g.ny;
       c.g.n = c.g.sxy * c.g.nz;
-      dx *= 2.0;
-      dy *= 2.0;
-      if (gf.dim == 3) dz *= 2.0;
       stride *= 2;
-      // exact coarse spacing from the domain, as the reference recomputes it
       const double cdx = (hp->xmax - hp->xmin) / (double)(c.g.nx - 1);
       const double cdy = (hp->ymax - hp->ymin) / (double)(c.g.ny - 1);
       const double cdz = gf.dim == 3 ? (hp->zmax - hp->zmin) / (double)(c.g.nz - 1) : 0.0;
       build_faces(ctx, hp, c.g.nx, c.g.ny, c.g.nz, cdx, cdy, cdz, stride, &c.g, &owned);
       c.cf = coarsen_coef(ctx, P, levels.back().cf, gf, c.g, cdx, cdy, cdz, &owned);
-      c.x = alloc(ctx, c.g.n);
+      c.xa = alloc(ctx, c.g.n);
+      c.xb = alloc(ctx, c.g.n);
       c.b = alloc(ctx, c.g.n);
       c.r = alloc(ctx, c.g.n);
       levels.push_back(c);
-      if (c.g.nx <= 5 || c.g.ny <= 5 || (c.g.dim == 3 && c.g.nz <= 5)) break;
+    }
+    // result buffer of each level after a V-cycle (fixed, so launches can be captured):
+    // the first sweep from zero writes xa, every later sweep flips the buffer
+    for (size_t l = 0; l < levels.size(); ++l) {
+      Level& L = levels[l];
+      if (!fused) {
+        L.out = L.xa;
+        continue;
+      }
+      int flips;
+      if (l + 1 == levels.size())
+        flips = coarse_in_smem(L) ? 0 : coarse_iters - 1;
+      else
+        flips = pre > 0 ? pre - 1 + post : post;
+      L.out = (flips & 1) ? L.xb : L.xa;
     }
   }
 
-  // one colour pass: 16 algorithmic bytes per interior node in FP64 (a full
-  // red+black sweep reads u, f, k and writes u once: 32 B/DOF)
-  void smooth(Context* ctx, const Level& L, const T* b, int sweeps, bool reverse, const Ctl* ctl, bool fine) {
-    const dim3 grid = stencil_grid(L.g), block = stencil_block();
-    const double bytes = interior_dofs(L.g) * 2.0 * sizeof(T);
-    for (int s = 0; s < sweeps; ++s) {
-      for (int half = 0; half < 2; ++half) {
-        ProfScope ps(ctx, "rbgs_color_pass", bytes, fine);
-        k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, L.x, (reverse ? 1 : 0) ^ half, ctl);
+  // `sweeps` red-black sweeps starting from `cur` (or from zero); returns the
+  // buffer holding the result. Two forms with identical arithmetic: colour
+  // passes in place (default), or fused single-pass sweeps that read one
+  // buffer and write the other.
+  bool fused = false;
+  T* sweeps_from(Context* ctx, Level& L, const T* b, T* cur, int sweeps, int first, bool from_zero,
+                 const Ctl* ctl, int lvl) {
+    const dim3 grid = stencil_grid_auto(L.g), block = stencil_block();
+    const double dofs = interior_dofs(L.g);
+    if (!fused) {
+      // in place: the buffer never changes; flips are bookkeeping only
+      if (from_zero) {
+        ProfScope ps(ctx, "zero_fill", lvl, dofs * sizeof(T));
+        vfill<T>(ctx, L.g.n, L.xa, T(0), ctl);
+        cur = L.xa;
       }
-      ctx->count(2);
+      for (int s = 0; s < sweeps; ++s) {
+        for (int half = 0; half < 2; ++half) {
+          ProfScope ps(ctx, "rbgs_color_pass", lvl, dofs * 2.0 * sizeof(T));
+          k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first ^ half, ctl);
+        }
+        ctx->count(2);
+      }
+      return cur;
     }
+    const dim3 fgrid = fused_grid(L.g);
+    for (int s = 0; s < sweeps; ++s) {
+      const bool zero = from_zero && s == 0;
+      T* in = zero ? L.xb : cur;
+      T* out = zero ? L.xa : (cur == L.xa ? L.xb : L.xa);
+      {
+        ProfScope ps(ctx, "rbgs_sweep", lvl, dofs * 4.0 * sizeof(T));
+        k_rbgs_fused<Coef, T, T><<<fgrid, block, 0, ctx->stream>>>(L.g, L.cf, b, in, out, first, zero ? 1 : 0, ctl);
+      }
+      ctx->count();
+      cur = out;
+    }
+    return cur;
   }
 
   void level(Context* ctx, int l, const T* rhs0, const Ctl* ctl) {
     Level& L = levels[l];
     const T* b = l == 0 ? rhs0 : L.b;
-    const bool fine = l == 0;
     const double dofs = interior_dofs(L.g);
-    {
-      ProfScope ps(ctx, "zero_fill", dofs * sizeof(T), fine);
-      vfill<T>(ctx, L.g.n, L.x, T(0), ctl);
-    }
     if (l == (int)levels.size() - 1) {
-      if (L.g.n <= 65536) {
-        k_coarse_solve<Coef, T, T><<<1, 256, 0, ctx->stream>>>(L.g, L.cf, b, L.x, coarse_iters, ctl);
+      if (coarse_in_smem(L)) {
+        ProfScope ps(ctx, "coarse_solve", l, 0.0);
+        k_coarse_solve_smem<Coef, T, T><<<1, 256, 0, ctx->stream>>>(L.g, L.cf, b, L.xa, coarse_iters, ctl);
         ctx->count();
       } else {
-        smooth(ctx, L, b, coarse_iters, false, ctl, fine);
+        T* cur = sweeps_from(ctx, L, b, L.xa, coarse_iters, 0, true, ctl, l);
+        (void)cur;
       }
       return;
     }
-    smooth(ctx, L, b, pre, false, ctl, fine);
+    T* cur = L.xa;
+    if (pre > 0) {
+      cur = sweeps_from(ctx, L, b, L.xa, pre, 0, true, ctl, l);
+    } else {
+      vfill<T>(ctx, L.g.n, L.xa, T(0), ctl);
+    }
     {
-      ProfScope ps(ctx, "residual", dofs * 4.0 * sizeof(T), fine);
-      k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(
-          L.g, L.cf, L.x, b, L.r, RedSlot{}, NoPost{}, ctl);
+      ProfScope ps(ctx, "residual", l, dofs * 4.0 * sizeof(T));
+      k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(
+          L.g, L.cf, cur, b, L.r, RedSlot{}, NoPost{}, ctl);
     }
     Level& C = levels[l + 1];
     {
-      ProfScope ps(ctx, "restrict", dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)), fine);
-      k_restrict<T, T><<<stencil_grid(C.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+      ProfScope ps(ctx, "restrict", l, dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
+      k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+    }
+    if (needs_fold) {
+      ProfScope ps(ctx, "restrict_fold", l, 0.0);
+      k_restrict_fold<T><<<stencil_grid_auto(C.g), stencil_block(), 0, ctx->stream>>>(C.g, C.b, ctl);
+      ctx->count();
     }
     ctx->count(2);
     level(ctx, l + 1, rhs0, ctl);
     {
-      ProfScope ps(ctx, "prolong_add", dofs * sizeof(T) * (2.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)), fine);
-      k_prolong_add<T, T><<<stencil_grid(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.x, L.x, ctl);
+      ProfScope ps(ctx, "prolong_add", l, dofs * sizeof(T) * (2.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
+      k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
     }
     ctx->count();
-    smooth(ctx, L, b, post, true, ctl, fine);
+    cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l);
   }
 
-  // z = M rhs0, result in levels[0].x
+  // z = M rhs0; the result is in levels[0].out
   void vcycle(Context* ctx, const T* rhs0, const Ctl* ctl) { level(ctx, 0, rhs0, ctl); }
+  T* z() const { return levels[0].out; }
 };
 
 // -------------------------------------------------- drivers in other units

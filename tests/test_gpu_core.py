@@ -153,3 +153,15 @@ def test_mgpcg_2d_poisson_matches_reference_cg_solution(oracle_mod):
     ref_opt = default_options(method=abi.CG, max_iter=8000, tol=1e-13)
     st, ref, _ = oracle_mod.rs_solve(p, ref_opt)
     assert rel_l2(got, ref) <= 1e-9
+
+
+def test_fused_sweep_form_matches_color_passes(monkeypatch):
+    # the single-pass red-black sweep and the two colour passes are the same
+    # arithmetic; results agree to rounding and iteration counts match
+    p = synthetic.varcoef_poisson_3d(33, seed=4)
+    opt = default_options(method=abi.MG_PCG, tol=1e-11, tol_mode=abi.TOL_RELATIVE, max_iter=200)
+    a, ra = solver.solve(p, opt)
+    monkeypatch.setenv("PDEB200_FUSED_SWEEP", "1")
+    b, rb = solver.solve(p, opt)
+    assert ra.iterations == rb.iterations
+    assert rel_l2(b, a) <= 1e-12

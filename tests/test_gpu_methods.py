@@ -1,0 +1,184 @@
+"""GPU parity of the remaining methods through the C ABI against the oracle
+(restatement pinned to the reference in tests/test_oracle_pins.py).
+
+Reference methods (lexicographic GS/SOR, single V-cycle, BiCGStab, GMRES,
+forward Euler, projection, residual norms) run the reference's algorithm:
+fields agree to rounding, rel L2 <= 1e-10 (FMA contraction is the only
+difference). B200 forms (MG-BiCGStab, mixed precision) are checked against
+FP64 solves of the same system: rel L2 <= 1e-9 at a 1e-12 residual."""
+import numpy as np
+import pytest
+
+from pde_solver_b200 import abi, solver, synthetic
+from pde_solver_b200.problem import FaceBC, GridProblem, default_options
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (d if d > 0 else 1.0)
+
+
+def faces_2d():
+    return [FaceBC.robin(1.0, 0.5, 0.2), FaceBC.dirichlet(0.0), FaceBC.neumann(0.3), FaceBC.dirichlet(1.0),
+            FaceBC(), FaceBC()]
+
+
+def faces_3d():
+    return [FaceBC.dirichlet(0.0), FaceBC.dirichlet(0.5), FaceBC.neumann(0.0), FaceBC.neumann(0.2),
+            FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(0.0)]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(lib):
+    return lib
+
+
+def _rhs(p, seed=2):
+    return np.random.Generator(np.random.PCG64(seed)).standard_normal(p.n)
+
+
+@pytest.mark.parametrize("method,omega", [(abi.GAUSS_SEIDEL, 1.0), (abi.SOR, 1.7)])
+@pytest.mark.parametrize("dims", [(25, 21, 1), (11, 9, 10)])
+def test_lexicographic_gs_sor(oracle_mod, method, omega, dims):
+    p = GridProblem(*dims, a=-1.0, b=-1.0, az=-1.0, c=0.4)
+    p.faces = faces_2d() if dims[2] == 1 else faces_3d()
+    p.f = _rhs(p)
+    opt = default_options(method=method, sor_omega=omega, max_iter=20000, tol=1e-11)
+    got, rep = solver.solve(p, opt)
+    st, ref, rrep = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rep.status == abi.OK
+    assert abs(rep.iterations - rrep.iterations) <= 1
+    assert rel_l2(got, ref) <= 1e-10
+
+
+def test_lexicographic_sor_loose_tol_same_iterate(oracle_mod):
+    # at the reference's default tolerance the field is far from converged; the
+    # exact ordering still reproduces it
+    p = GridProblem(33, 33, 1, a=-1.0, b=-1.0)
+    p.faces = faces_2d()
+    p.f = _rhs(p, 5)
+    opt = default_options(method=abi.SOR, sor_omega=1.5, max_iter=10000, tol=1e-6)
+    got, rep = solver.solve(p, opt)
+    st, ref, rrep = oracle_mod.rs_solve(p, opt)
+    assert rep.iterations == rrep.iterations
+    assert rel_l2(got, ref) <= 1e-12
+
+
+def test_reference_single_vcycle(oracle_mod):
+    p = GridProblem(65, 33, 1, a=-1.0, b=-1.0)
+    p.faces = [FaceBC.dirichlet(0.0), FaceBC.dirichlet(1.0), FaceBC.dirichlet(0.0), FaceBC.dirichlet(2.0),
+               FaceBC(), FaceBC()]
+    p.f = _rhs(p, 7)
+    opt = default_options(method=abi.MG_VCYCLE)
+    got, _ = solver.solve(p, opt)
+    st, ref, _ = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("method,restart", [(abi.BICGSTAB, 30), (abi.GMRES, 400)])
+def test_reference_nonsymmetric_krylov(oracle_mod, method, restart):
+    p = GridProblem(21, 19, 1, a=-1.0, b=-0.5, c=3.0, d=-2.0, e=-0.3)
+    p.faces = [FaceBC.dirichlet(0.5), FaceBC.dirichlet(0.0), FaceBC.dirichlet(1.0), FaceBC.dirichlet(0.0),
+               FaceBC(), FaceBC()]
+    p.f = _rhs(p, 3)
+    opt = default_options(method=method, max_iter=3000, tol=1e-10, gmres_restart=restart)
+    got, rep = solver.solve(p, opt)
+    st, ref, rrep = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rep.status == abi.OK
+    assert rel_l2(got, ref) <= 1e-9
+
+
+def test_gmres_restart_defect_reproduced(oracle_mod):
+    p = GridProblem(33, 29, 1, a=-1.0, b=-0.5, c=3.0, d=-2.0, e=-0.3)
+    p.f = _rhs(p, 4)
+    opt = default_options(method=abi.GMRES, max_iter=3000, tol=1e-10, gmres_restart=25)
+    got, rep = solver.solve(p, opt, raise_on_error=False)
+    st, _, _ = oracle_mod.rs_solve(p, opt)
+    assert st != abi.OK and rep.status != abi.OK
+
+
+def test_bicgstab_3d(oracle_mod):
+    p = GridProblem(17, 15, 13, a=-1.0, b=-1.0, az=-1.0, c=1.0, dz=-0.5)
+    p.f = _rhs(p, 8)
+    opt = default_options(method=abi.BICGSTAB, max_iter=2000, tol=1e-10)
+    got, rep = solver.solve(p, opt)
+    st, ref, _ = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rel_l2(got, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("dims", [(33, 29, 1), (13, 12, 11)])
+def test_forward_euler_series(oracle_mod, dims):
+    p = GridProblem(*dims, a=-1.0, b=-1.0, az=-1.0, ut=1.0)
+    p.faces = faces_2d() if dims[2] == 1 else faces_3d()
+    x, y, z = p.coords()
+    p.u0 = (np.exp(-40 * ((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2 * (dims[2] > 1)))).reshape(-1)
+    h = min(1.0 / (d - 1) for d in dims if d > 1)
+    dim = 3 if dims[2] > 1 else 2
+    dt = 0.9 * h * h / (2 * dim)
+    frames_seen = []
+    got, rep = solver.time_series(p, 0.0, dt, 40, on_frame=lambda f, t, g: frames_seen.append(f))
+    ref, ref_frames = oracle_mod.rs_time_series(p, 0.0, dt, 40, keep_frames=True)
+    assert frames_seen == list(range(40))
+    assert rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("dims", [(48, 40, 1), (16, 14, 12)])
+def test_projection(oracle_mod, dims):
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    rng = np.random.Generator(np.random.PCG64(21))
+    u, v = rng.standard_normal(n), rng.standard_normal(n)
+    w = rng.standard_normal(n) if nz > 1 else None
+    p = np.zeros(n)
+    dx, dy, dz = 1.0 / (nx - 1), 1.0 / (ny - 1), (1.0 / (nz - 1) if nz > 1 else 1.0)
+    ug, vg, wg, pg, rep = solver.project_velocity(u, v, w, p, nx, ny, nz, dx, dy, dz, 0.01, 4000, 1e-10)
+    st, ur, vr, wr, pr, rrep = oracle_mod.rs_project(u, v, w, p, nx, ny, nz, dx, dy, dz, 0.01, 4000, 1e-10)
+    assert st == 0 and rep.status == abi.OK and rep.success == 1
+    assert abs(rep.poisson_iterations - rrep.poisson_iterations) <= 2
+    for a, b in ((ug, ur), (vg, vr), (pg, pr)):
+        assert rel_l2(a, b) <= 1e-8
+    # the reported divergence norms follow the oracle's
+    assert rep.max_divergence_before == pytest.approx(rrep.max_divergence_before, rel=1e-12)
+    assert rep.l2_divergence_before == pytest.approx(rrep.l2_divergence_before, rel=1e-12)
+    assert rep.max_divergence_after == pytest.approx(rrep.max_divergence_after, rel=1e-6)
+    assert rep.l2_divergence_after == pytest.approx(rrep.l2_divergence_after, rel=1e-6)
+
+
+@pytest.mark.parametrize("dims", [(19, 17, 1), (9, 8, 7)])
+def test_residual_norms(oracle_mod, dims):
+    p = GridProblem(*dims, a=-1.0, b=-2.0, az=-1.0, c=0.3, e=0.2, f_const=0.7)
+    p.faces = [FaceBC.robin(1.0, 0.5, 0.2), FaceBC.robin(2.0, 0.25, 0.1), FaceBC.neumann(0.3),
+               FaceBC.dirichlet(1.0), FaceBC.dirichlet(0.0), FaceBC.neumann(0.1)]
+    grid = np.random.Generator(np.random.PCG64(3)).standard_normal(p.n)
+    l2, linf = solver.residual_norms(p, grid)
+    rl2, rlinf = oracle_mod.rs_residual_norms(p, grid)
+    assert l2 == pytest.approx(rl2, rel=1e-12)
+    assert linf == pytest.approx(rlinf, rel=1e-12)
+
+
+def test_mg_bicgstab_convection_diffusion(oracle_mod):
+    # eps = 0.16 at h = 1/32 gives the fine-grid cell Peclet number of the
+    # 513^3, eps = 1e-2 workload (about 0.1)
+    p = synthetic.convection_diffusion_3d(33, seed=99, eps=0.16)
+    opt = default_options(method=abi.MG_BICGSTAB, tol=1e-12, tol_mode=abi.TOL_RELATIVE, max_iter=300)
+    got, rep = solver.solve(p, opt)
+    assert rep.status == abi.OK and rep.rel_residual <= 1e-11
+    ref_opt = default_options(method=abi.BICGSTAB, tol=1e-13, max_iter=20000)
+    st, ref, _ = oracle_mod.rs_solve(p, ref_opt)
+    assert st == 0 and rel_l2(got, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("method,bf16", [(abi.MG_PCG, 0), (abi.MG_PCG, 1), (abi.MG_BICGSTAB, 0)])
+def test_mixed_precision_refinement(method, bf16):
+    p = synthetic.varcoef_poisson_3d(33, seed=6)
+    if method == abi.MG_BICGSTAB:
+        p.c, p.d, p.dz = 0.6, -0.3, 0.2
+    fp64, r64 = solver.solve(p, default_options(method=method, tol=1e-12, tol_mode=abi.TOL_RELATIVE, max_iter=300))
+    mixed, rm = solver.solve(p, default_options(method=method, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=300,
+                                                precision=abi.MIXED, inner_tol=1e-4, bf16_coefficients=bf16))
+    assert rm.status == abi.OK
+    assert rm.rel_residual <= 1e-10          # FP64 true residual of the refined result
+    assert rm.outer_iterations >= 2
+    assert rel_l2(mixed, fp64) <= 1e-8       # error vs the FP64 solution
