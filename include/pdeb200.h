@@ -299,6 +299,25 @@ pdeb200_status pdeb200_project_velocity(int32_t nx, int32_t ny, int32_t nz,
                                         const pdeb200_projection_options* popt,
                                         pdeb200_projection_report* report);
 
+/* ---- solve without device allocation ----------------------------------- */
+
+/* No counterpart in the reference: an addition for callers that cannot let a
+ * library allocate device memory (code running inside another runtime's fixed
+ * memory arena, hosts that forbid allocation after start-up). Runs the Jacobi
+ * method with pdeb200_solve's semantics, but allocates nothing: the problem's
+ * k / nodal / f arrays and out_grid are device pointers (mem_space DEVICE),
+ * faces take constant values only, and the solver's scratch (second field,
+ * reduction partials, control block) is one file-scope device array of about
+ * 8.3 MB that every GPU loading the library keeps until the process exits.
+ * Grids above 1048576 nodes are rejected (PDEB200_ERR_UNSUPPORTED). All calls
+ * share that array: calls that overlap on the GPU race, so callers serialise
+ * them. The first call on a device looks up the array's address (set-up) and
+ * should come before any stream capture on that device. `stream` may be NULL
+ * (the default stream). */
+pdeb200_status pdeb200_jacobi_noalloc(const pdeb200_problem* prob, int32_t max_iter, double tol,
+                                      int32_t device, void* stream, double* out_grid,
+                                      pdeb200_report* report);
+
 #ifdef __cplusplus
 }
 #endif

@@ -197,6 +197,9 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_profile_enable.argtypes = [C.c_int32, C.c_int32]
     lib.pdeb200_profile_read.restype = C.c_int32
     lib.pdeb200_profile_read.argtypes = [C.c_int32, P(KernelStat), C.c_int32]
+    lib.pdeb200_jacobi_noalloc.restype = C.c_int32
+    lib.pdeb200_jacobi_noalloc.argtypes = [P(Problem), C.c_int32, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
+                                           P(Report)]
     return lib
 
 
