@@ -1,0 +1,38 @@
+"""Run the benchmark workloads through the C ABI without timing harness:
+
+    python -m pde_solver_b200.workload --n 257 --solves 2 [--method MG_PCG] [--mixed]
+
+Used as the target of profiler runs (each solve is the step `bench.py` times).
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+from . import abi, solver, synthetic
+from .problem import default_options
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=257)
+    ap.add_argument("--solves", type=int, default=2)
+    ap.add_argument("--method", default="MG_PCG", choices=["MG_PCG", "MG_BICGSTAB", "CG", "JACOBI"])
+    ap.add_argument("--mixed", action="store_true")
+    ap.add_argument("--workload", default="varcoef3d", choices=["varcoef3d", "convdiff3d"])
+    a = ap.parse_args(argv)
+    if a.workload == "varcoef3d":
+        p = synthetic.varcoef_poisson_3d(a.n, seed=1234)
+    else:
+        p = synthetic.convection_diffusion_3d(a.n, seed=99)
+    opt = default_options(method=getattr(abi, a.method), tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400,
+                          precision=abi.MIXED if a.mixed else abi.FP64)
+    for _ in range(a.solves):
+        _, rep = solver.solve(p, opt)
+        print(f"iterations={rep.iterations} outer={rep.outer_iterations} rel_residual={rep.rel_residual:.3e} "
+              f"device_ms={rep.device_ms:.2f} launches={rep.kernel_launches}", flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
