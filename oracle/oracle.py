@@ -216,3 +216,74 @@ def ref_project(u, v, w, p, nx, ny, nz, dx, dy, dz, dt, max_iter=1000, tol=1e-8,
     st = reference().pderef_project(nx, ny, nz, dx, dy, dz, dt, _dp(u), _dp(v), _dp(w), _dp(p),
                                     max_iter, tol, fix_corner, _dp(rep))
     return st, u, v, w, p, rep
+
+
+# ------------------------------------------------------------ drop-in harness
+
+DROPIN_SO = os.path.join(HERE, "_ref", "libdropin.so")
+_dropin = None
+
+
+def have_dropin() -> bool:
+    return os.path.exists(DROPIN_SO)
+
+
+def dropin() -> C.CDLL:
+    """oracle/_ref/libdropin.so: the reference's SolveWithBackend with its CUDA
+    backend served by pde_solver_b200/shim/cuda_solver_shim.cpp."""
+    global _dropin
+    if _dropin is None:
+        lib = C.CDLL(DROPIN_SO)
+        cpp = P(C.c_char_p)
+        lib.dropin_solve_with_backend.restype = C.c_int
+        lib.dropin_solve_with_backend.argtypes = [P(abi.Problem), C.c_char_p, cpp, cpp, P(abi.Options), C.c_int, DP,
+                                                  DP, DP, P(C.c_int), C.c_char_p, C.c_size_t]
+        lib.dropin_solve_cuda.restype = C.c_int
+        lib.dropin_solve_cuda.argtypes = [P(abi.Problem), C.c_char_p, cpp, cpp, P(abi.Options), DP, C.c_char_p,
+                                          C.c_size_t]
+        lib.dropin_time_series_cuda.restype = C.c_int
+        lib.dropin_time_series_cuda.argtypes = [P(abi.Problem), C.c_char_p, C.c_double, C.c_double, C.c_int, DP, DP,
+                                                C.c_char_p, C.c_size_t]
+        lib.dropin_probe.restype = C.c_int
+        lib.dropin_probe.argtypes = [C.c_char_p, C.c_size_t]
+        _dropin = lib
+    return _dropin
+
+
+def _cstrs(items, count):
+    if items is None:
+        return None
+    arr = (C.c_char_p * count)(*[(s.encode() if s else None) for s in items])
+    return C.cast(arr, P(C.c_char_p))
+
+
+def dropin_solve(prob, opt, backend, rhs_latex=None, coef_latex=None, face_latex=None):
+    """backend 1 = CUDA (the B200 shim), 0 = CPU; returns (status, grid, (l2, linf), selected_cuda, error)."""
+    out = np.zeros(prob.n)
+    l2, linf = C.c_double(), C.c_double()
+    sel = C.c_int(-1)
+    err = C.create_string_buffer(512)
+    cp = prob.to_c()
+    st = dropin().dropin_solve_with_backend(C.byref(cp), rhs_latex.encode() if rhs_latex else None,
+                                            _cstrs(coef_latex, 7), _cstrs(face_latex, 6), C.byref(opt), backend,
+                                            _dp(out), C.byref(l2), C.byref(linf), C.byref(sel), err, 512)
+    return st, out, (l2.value, linf.value), sel.value == 1, err.value.decode()
+
+
+def dropin_solve_cuda(prob, opt, rhs_latex=None, coef_latex=None, face_latex=None):
+    out = np.zeros(prob.n)
+    err = C.create_string_buffer(512)
+    cp = prob.to_c()
+    st = dropin().dropin_solve_cuda(C.byref(cp), rhs_latex.encode() if rhs_latex else None, _cstrs(coef_latex, 7),
+                                    _cstrs(face_latex, 6), C.byref(opt), _dp(out), err, 512)
+    return st, out, err.value.decode()
+
+
+def dropin_time_series_cuda(prob, t_start, dt, frames, rhs_latex=None):
+    out = np.zeros(prob.n)
+    fr = np.zeros(prob.n * frames)
+    err = C.create_string_buffer(512)
+    cp = prob.to_c()
+    st = dropin().dropin_time_series_cuda(C.byref(cp), rhs_latex.encode() if rhs_latex else None, t_start, dt, frames,
+                                          _dp(out), _dp(fr), err, 512)
+    return st, out, fr.reshape(frames, -1), err.value.decode()

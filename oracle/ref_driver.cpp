@@ -11,6 +11,9 @@
 //   ProjectVelocity2D / ProjectVelocity3D          src/pressure_projection.cpp:255,698
 //   ComputeResidualNorms                           src/residual.cpp:153
 //   RunSelfTest                                    src/self_test.cpp:224
+// Built with PDEREF_DROPIN (oracle/_ref/libdropin.so) it also drives the
+// reference's SolveWithBackend with the CUDA backend compiled in and served by
+// the B200 shim (pde_solver_b200/shim/cuda_solver_shim.cpp).
 #include <omp.h>
 
 #include <cstring>
@@ -25,6 +28,11 @@
 #include "residual.h"
 #include "self_test.h"
 #include "solver.h"
+#ifdef PDEREF_DROPIN
+#include "cuda_solver.h"
+SolveOutput SolvePDETimeSeriesCuda(const SolveInput& input, const FrameCallback& on_frame,
+                                   const ProgressCallback& progress);
+#endif
 
 namespace {
 
@@ -286,7 +294,99 @@ int pderef_project(int nx, int ny, int nz, double dx, double dy, double dz, doub
 }
 
 // The reference's own analytic self-test (src/self_test.cpp:224-411); returns
-// its failure count.
+// 1 when any case fails.
 int pderef_self_test(void) { return RunSelfTest(); }
+
+#ifdef PDEREF_DROPIN
+// Drop-in harness: the same SolveInput through the reference's dispatch with
+// the CUDA backend compiled in (USE_CUDA) and served by the B200 shim.
+int dropin_solve_with_backend(const pdeb200_problem* p, const char* rhs_latex, const char* const* coef_latex,
+                              const char* const* face_value_latex, const pdeb200_options* o, int backend,
+                              double* out, double* resid_l2, double* resid_linf, int* selected, char* err,
+                              size_t err_len) {
+  SolveInput in;
+  std::string error;
+  if (!BuildInput(p, rhs_latex, coef_latex, &in, &error)) {
+    CopyError(error, err, err_len);
+    return 1;
+  }
+  if (face_value_latex) {
+    BoundaryCondition* bcs[6] = {&in.bc.left, &in.bc.right, &in.bc.bottom, &in.bc.top, &in.bc.front, &in.bc.back};
+    for (int f = 0; f < 6; ++f)
+      if (face_value_latex[f]) bcs[f]->value.latex = face_value_latex[f];
+  }
+  ApplyOptions(o, &in);
+  BackendKind sel = BackendKind::CPU;
+  std::string note;
+  SolveOutput res = SolveWithBackend(in, backend == 1 ? BackendKind::CUDA : BackendKind::CPU, &sel, &note);
+  if (selected) *selected = sel == BackendKind::CUDA ? 1 : 0;
+  if (!res.error.empty()) {
+    CopyError(res.error, err, err_len);
+    return 2;
+  }
+  std::memcpy(out, res.grid.data(), res.grid.size() * sizeof(double));
+  if (resid_l2) *resid_l2 = res.residual_l2;
+  if (resid_linf) *resid_linf = res.residual_linf;
+  return 0;
+}
+
+// SolvePDECuda directly (the reference's capability gate keeps CUDA to 2D).
+int dropin_solve_cuda(const pdeb200_problem* p, const char* rhs_latex, const char* const* coef_latex,
+                      const char* const* face_value_latex, const pdeb200_options* o, double* out, char* err,
+                      size_t err_len) {
+  SolveInput in;
+  std::string error;
+  if (!BuildInput(p, rhs_latex, coef_latex, &in, &error)) {
+    CopyError(error, err, err_len);
+    return 1;
+  }
+  if (face_value_latex) {
+    BoundaryCondition* bcs[6] = {&in.bc.left, &in.bc.right, &in.bc.bottom, &in.bc.top, &in.bc.front, &in.bc.back};
+    for (int f = 0; f < 6; ++f)
+      if (face_value_latex[f]) bcs[f]->value.latex = face_value_latex[f];
+  }
+  ApplyOptions(o, &in);
+  SolveOutput res = SolvePDECuda(in);
+  if (!res.error.empty()) {
+    CopyError(res.error, err, err_len);
+    return 2;
+  }
+  std::memcpy(out, res.grid.data(), res.grid.size() * sizeof(double));
+  return 0;
+}
+
+int dropin_time_series_cuda(const pdeb200_problem* p, const char* rhs_latex, double t_start, double dt, int frames,
+                            double* out, double* frames_out, char* err, size_t err_len) {
+  SolveInput in;
+  std::string error;
+  if (!BuildInput(p, rhs_latex, nullptr, &in, &error)) {
+    CopyError(error, err, err_len);
+    return 1;
+  }
+  in.time.enabled = true;
+  in.time.t_start = t_start;
+  in.time.dt = dt;
+  in.time.frames = frames;
+  const size_t n = static_cast<size_t>(p->nx) * p->ny * (p->nz <= 1 ? 1 : p->nz);
+  FrameCallback cb = [&](int frame, double, const std::vector<double>& grid, const std::vector<double>*) -> bool {
+    if (frames_out) std::memcpy(frames_out + static_cast<size_t>(frame) * n, grid.data(), n * sizeof(double));
+    return true;
+  };
+  SolveOutput res = SolvePDETimeSeriesCuda(in, cb, ProgressCallback());
+  if (!res.error.empty()) {
+    CopyError(res.error, err, err_len);
+    return 2;
+  }
+  std::memcpy(out, res.grid.data(), n * sizeof(double));
+  return 0;
+}
+
+int dropin_probe(char* note, size_t len) {
+  std::string s;
+  const bool ok = CudaIsAvailable(&s);
+  CopyError(s, note, len);
+  return ok ? 1 : 0;
+}
+#endif
 
 }  // extern "C"
