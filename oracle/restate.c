@@ -926,9 +926,10 @@ static void fill_boundary(const Grid* g, double* u) {
 /* ---------------------------------------------------- MG hierarchy (B200) */
 
 /* Geometric hierarchy of the folded operator: vertex-centred coarsening
- * n_c = (n+1)/2 while every active dimension is odd and >= 5 (the coarsening
- * of multigrid.cpp:150-170, continued down to 3 nodes), coarse k by
- * injection, faces and h rediscretised. */
+ * n_c = ceil((n-1)/2) + 1 per dimension (coarse_dims; for odd cubes the 2:1
+ * coarsening of multigrid.cpp:150-170, continued down to 3 nodes; even n gives
+ * non-nested levels), coarse k from the nearest fine
+ * node, faces sampled at the nearest finest-level face node, h rediscretised. */
 typedef struct {
   Grid g;
   pdeb200_problem p;
@@ -936,10 +937,33 @@ typedef struct {
   double *x, *b, *r;
 } Level;
 
-static int can_coarsen(const Grid* g) {
-  if (!(g->nx >= 5 && g->nx % 2 == 1 && g->ny >= 5 && g->ny % 2 == 1)) return 0;
-  if (g->dim == 3 && !(g->nz >= 5 && g->nz % 2 == 1)) return 0;
-  return 1;
+static int coarse_size(int n) { return n / 2 + 1; } /* ceil((n-1)/2) + 1 */
+
+/* Per-dimension coarsening: a dimension with >= 5 nodes coarsens when its
+ * spacing is below twice the smallest spacing (semi-coarsening on elongated
+ * grids); 0 when none does. */
+static int coarse_dims(const Grid* g, int nc[3]) {
+  const int n[3] = {g->nx, g->ny, g->nz};
+  const double h[3] = {g->dx, g->dy, g->dz};
+  const int dims = g->dim == 3 ? 3 : 2;
+  double hmin = h[0];
+  int any = 0;
+  for (int d = 1; d < dims; ++d)
+    if (h[d] < hmin) hmin = h[d];
+  for (int d = 0; d < 3; ++d) {
+    nc[d] = n[d];
+    if (d < dims && n[d] >= 5 && h[d] < 2.0 * hmin) {
+      nc[d] = coarse_size(n[d]);
+      any = 1;
+    }
+  }
+  return any;
+}
+
+/* nearest fine node of coarse node I (coarse I sits at I*(n-1)/(nc-1)) */
+static int nearest_fine(int I, int n, int nc) {
+  if (nc <= 1) return 0;
+  return (I * (n - 1) + (nc - 1) / 2) / (nc - 1);
 }
 
 static int build_levels(const Grid* g0, int max_levels, Level* lv) {
@@ -951,25 +975,28 @@ static int build_levels(const Grid* g0, int max_levels, Level* lv) {
   L = 1;
   while (L < max_levels && L < 16) {
     const Grid* pg = &lv[L - 1].g;
-    if (!can_coarsen(pg)) break;
+    int nc[3];
+    if (!coarse_dims(pg, nc)) break;
     Level* c = &lv[L];
     c->p = lv[L - 1].p;
-    c->p.nx = (pg->nx + 1) / 2;
-    c->p.ny = (pg->ny + 1) / 2;
-    c->p.nz = pg->dim == 3 ? (pg->nz + 1) / 2 : 1;
-    /* coarse faces: constants only (per-node face arrays are sampled by injection) */
+    c->p.nx = nc[0];
+    c->p.ny = nc[1];
+    c->p.nz = pg->dim == 3 ? nc[2] : 1;
+    /* coarse faces: constants only (per-node face arrays are sampled below) */
     for (int f = 0; f < 6; ++f) {
       c->p.face[f].value_arr = c->p.face[f].alpha_arr = c->p.face[f].beta_arr = c->p.face[f].gamma_arr = NULL;
     }
     if (grid_init(&c->g, &c->p) != PDEB200_OK) break;
     for (int f = 0; f < 6; ++f) {
-      const Grid* fg = pg;
+      const Grid* fg = &lv[0].g;
+      const int w = f <= RIGHT ? c->g.ny : c->g.nx;
+      const int h = f <= RIGHT ? c->g.nz : (f <= TOP ? c->g.nz : c->g.ny);
+      const int fw = f <= RIGHT ? fg->ny : fg->nx;
+      const int fh = f <= RIGHT ? fg->nz : (f <= TOP ? fg->nz : fg->ny);
       for (int q = 0; q < c->g.fsize[f]; ++q) {
-        /* inject face parameters: coarse face node (a,b) <- fine (2a,2b) */
-        const int w = f <= RIGHT ? c->g.ny : c->g.nx;
-        const int fw = f <= RIGHT ? fg->ny : fg->nx;
+        /* face parameters: coarse face node (a,b) <- nearest finest face node */
         const int qa = q % w, qb = q / w;
-        const int fq = 2 * qa + fw * (2 * qb);
+        const int fq = nearest_fine(qa, fw, w) + fw * nearest_fine(qb, fh, h);
         c->g.val[f][q] = fg->val[f][fq];
         c->g.al[f][q] = fg->al[f][fq];
         c->g.be[f][q] = fg->be[f][fq];
@@ -983,7 +1010,9 @@ static int build_levels(const Grid* g0, int max_levels, Level* lv) {
       for (int k = 0; k < c->g.nz; ++k)
         for (int j = 0; j < c->g.ny; ++j)
           for (int i = 0; i < c->g.nx; ++i)
-            c->k[ID(&c->g, i, j, k)] = lv[L - 1].k[ID(pg, 2 * i, 2 * j, pg->dim == 3 ? 2 * k : 0)];
+            c->k[ID(&c->g, i, j, k)] =
+                lv[L - 1].k[ID(pg, nearest_fine(i, pg->nx, c->g.nx), nearest_fine(j, pg->ny, c->g.ny),
+                               pg->dim == 3 ? nearest_fine(k, pg->nz, c->g.nz) : 0)];
       c->p.k = c->k;
     }
     c->p.f = NULL;
@@ -995,6 +1024,36 @@ static int build_levels(const Grid* g0, int max_levels, Level* lv) {
     lv[l].r = calloc(lv[l].g.n, sizeof(double));
   }
   return L;
+}
+
+/* Interpolation position of fine node i: coarse interval I0 and weight t of
+ * node I0+1 (exact rational position i*(nc-1)/(n-1)). */
+static void coarse_pos(int i, int n, int nc, int* I0, double* t) {
+  const int num = i * (nc - 1);
+  *I0 = num / (n - 1);
+  *t = (double)(num - *I0 * (n - 1)) / (double)(n - 1);
+  if (*I0 >= nc - 1) {
+    *I0 = nc - 1;
+    *t = 0.0;
+  }
+}
+
+/* Restriction weights (scaled transpose of the interpolation) of coarse node
+ * I: w_i = (nc-1)/(n-1) * max(0, 1 - |i(nc-1) - I(n-1)|/(n-1)). */
+static int restrict_weights(int I, int n, int nc, int* idx, double* w) {
+  const int den = n - 1;
+  const double scale = (double)(nc - 1) / (double)den;
+  int cnt = 0;
+  for (int i = 0; i < n; ++i) {
+    int d = i * (nc - 1) - I * den;
+    if (d < 0) d = -d;
+    if (d < den) {
+      idx[cnt] = i;
+      w[cnt] = scale * (1.0 - (double)d / (double)den);
+      ++cnt;
+    }
+  }
+  return cnt;
 }
 
 static void free_levels(Level* lv, int L) {
@@ -1136,8 +1195,9 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   /* r = b - A x */
   folded_apply(g, x, lv[l].r);
   for (long q = 0; q < g->n; ++q) lv[l].r[q] = b[q] - lv[l].r[q];
-  /* full weighting r -> coarse b (tensor [1/4,1/2,1/4]) at every coarse node
-   * (in-range fine neighbours), then the transpose of the boundary extension
+  /* full weighting r -> coarse b (tensor [1/4,1/2,1/4] for odd n, the scaled
+   * transpose of the interpolation in general) at every coarse node, then the
+   * transpose of the boundary extension
    * folds the boundary-node values into the interior: R = Ext^T P^T / 2^dim. */
   Grid* c = &lv[l + 1].g;
   double* bc = lv[l + 1].b;
@@ -1145,20 +1205,27 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   const int all = g_mg_boundary_transfer;
   const int kc0 = c->dim == 3 ? (all ? 0 : 1) : 0, kc1 = c->dim == 3 ? (all ? c->nz : c->nz - 1) : 1;
   const int ic0 = all ? 0 : 1, ic1 = all ? c->nx : c->nx - 1, jc0 = all ? 0 : 1, jc1 = all ? c->ny : c->ny - 1;
-  const double wt[3] = {0.25, 0.5, 0.25};
   for (int K = kc0; K < kc1; ++K)
     for (int J = jc0; J < jc1; ++J)
       for (int I = ic0; I < ic1; ++I) {
+        int ix[4], iy[4], iz[4];
+        double wx[4], wy[4], wz[4];
+        const int nxw = restrict_weights(I, g->nx, c->nx, ix, wx);
+        const int nyw = restrict_weights(J, g->ny, c->ny, iy, wy);
+        int nzw = 1;
+        if (c->dim == 3) {
+          nzw = restrict_weights(K, g->nz, c->nz, iz, wz);
+        } else {
+          iz[0] = 0;
+          wz[0] = 1.0;
+        }
         double acc = 0.0;
-        const int dk0 = c->dim == 3 ? -1 : 0, dk1 = c->dim == 3 ? 1 : 0;
-        for (int dk = dk0; dk <= dk1; ++dk)
-          for (int dj = -1; dj <= 1; ++dj)
-            for (int di = -1; di <= 1; ++di) {
-              const int fi = 2 * I + di, fj = 2 * J + dj, fk = c->dim == 3 ? 2 * K + dk : 0;
-              if (fi < 0 || fi >= g->nx || fj < 0 || fj >= g->ny || fk < 0 || fk >= g->nz) continue;
-              const double w = wt[di + 1] * wt[dj + 1] * (c->dim == 3 ? wt[dk + 1] : 1.0);
-              acc += w * lv[l].r[ID(g, fi, fj, fk)];
-            }
+        for (int cc = 0; cc < nzw; ++cc)
+          for (int bb = 0; bb < nyw; ++bb) {
+            double rs = 0.0;
+            for (int aa = 0; aa < nxw; ++aa) rs += wx[aa] * lv[l].r[ID(g, ix[aa], iy[bb], iz[cc])];
+            acc += wz[cc] * wy[bb] * rs;
+          }
         bc[ID(c, I, J, K)] = acc;
       }
   if (all) ext_transpose(c, bc);
@@ -1172,11 +1239,19 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   for (int k = kf0; k < kf1; ++k)
     for (int j = 1; j < g->ny - 1; ++j)
       for (int i = 1; i < g->nx - 1; ++i) {
-        const int I0 = i / 2, I1 = (i + 1) / 2, J0 = j / 2, J1 = (j + 1) / 2;
-        const int K0 = g->dim == 3 ? k / 2 : 0, K1 = g->dim == 3 ? (k + 1) / 2 : 0;
-        const double v = 0.125 * (xc[ID(c, I0, J0, K0)] + xc[ID(c, I1, J0, K0)] + xc[ID(c, I0, J1, K0)] +
-                                  xc[ID(c, I1, J1, K0)] + xc[ID(c, I0, J0, K1)] + xc[ID(c, I1, J0, K1)] +
-                                  xc[ID(c, I0, J1, K1)] + xc[ID(c, I1, J1, K1)]);
+        int I0, J0, K0 = 0;
+        double tx, ty, tz = 0.0;
+        coarse_pos(i, g->nx, c->nx, &I0, &tx);
+        coarse_pos(j, g->ny, c->ny, &J0, &ty);
+        if (g->dim == 3) coarse_pos(k, g->nz, c->nz, &K0, &tz);
+        const int I1 = I0 + 1 < c->nx ? I0 + 1 : c->nx - 1, J1 = J0 + 1 < c->ny ? J0 + 1 : c->ny - 1;
+        const int K1 = g->dim == 3 ? (K0 + 1 < c->nz ? K0 + 1 : c->nz - 1) : 0;
+        const double x00 = (1.0 - tx) * xc[ID(c, I0, J0, K0)] + tx * xc[ID(c, I1, J0, K0)];
+        const double x10 = (1.0 - tx) * xc[ID(c, I0, J1, K0)] + tx * xc[ID(c, I1, J1, K0)];
+        const double x01 = (1.0 - tx) * xc[ID(c, I0, J0, K1)] + tx * xc[ID(c, I1, J0, K1)];
+        const double x11 = (1.0 - tx) * xc[ID(c, I0, J1, K1)] + tx * xc[ID(c, I1, J1, K1)];
+        const double y0 = (1.0 - ty) * x00 + ty * x10, y1 = (1.0 - ty) * x01 + ty * x11;
+        const double v = (1.0 - tz) * y0 + tz * y1;
         x[ID(g, i, j, k)] += v;
       }
   for (int it = 0; it < post; ++it) {

@@ -603,29 +603,100 @@ __device__ __forceinline__ long long cidx(const GridDev& g, int i, int j, int k)
   return ((long long)k * g.ny + j) * g.nx + i;
 }
 
-// Full weighting (tensor [1/4,1/2,1/4]) of the fine residual at coarse node
-// (I,J,K), boundary coarse nodes included (fine neighbours outside the grid
-// do not exist; fine boundary values of the residual are zero).
+// Transfer maps for any fine/coarse pair n -> nc per dimension: coarse node I
+// sits at fine position I*(n-1)/(nc-1). Three forms, chosen per dimension:
+// identity (nc = n, semi-coarsening), nested 2:1 (n odd, nc = (n+1)/2) and
+// general (n even, nc = n/2 + 1). The nested form is the general formula
+// evaluated exactly (weights 1/2 and 1/4 are exact), so the forms agree bit
+// for bit where they overlap.
+__device__ __forceinline__ int map_mode(int n, int nc) { return nc == n ? 0 : (2 * nc - 1 == n ? 1 : 2); }
+
+// Interpolation position of fine node i: coarse interval I0 and weight t of
+// node I0 + 1 (t = 0 on coincident nodes).
+__device__ __forceinline__ void coarse_pos(int i, int n, int nc, int mode, int& I0, double& t) {
+  if (mode == 0) {
+    I0 = i;
+    t = 0.0;
+    return;
+  }
+  if (mode == 1) {
+    I0 = i >> 1;
+    t = (i & 1) ? 0.5 : 0.0;
+    return;
+  }
+  const int num = i * (nc - 1);
+  I0 = num / (n - 1);
+  const int rem = num - I0 * (n - 1);
+  t = double(rem) / double(n - 1);
+  if (I0 >= nc - 1) {
+    I0 = nc - 1;
+    t = 0.0;
+  }
+}
+
+// Restriction weights of coarse node I over fine nodes, the scaled transpose
+// of the interpolation: w_i = (nc-1)/(n-1) * max(0, 1 - |i(nc-1) - I(n-1)|/(n-1))
+// ({1/4, 1/2, 1/4} for the nested form). Always four consecutive entries
+// (i0 .. i0+3); entries outside the grid or the support carry weight 0 and a
+// clamped index.
+__device__ __forceinline__ void restrict_weights(int I, int n, int nc, int mode, int& i0, double (&w)[4]) {
+  if (mode == 0) {
+    i0 = I;
+    w[0] = 1.0;
+    w[1] = w[2] = w[3] = 0.0;
+    return;
+  }
+  if (mode == 1) {
+    i0 = 2 * I - 1;
+    w[0] = 0.25;
+    w[1] = 0.5;
+    w[2] = 0.25;
+    w[3] = 0.0;
+  } else {
+    const int den = n - 1, m = nc - 1;
+    const int num = (I - 1) * den;
+    const int fl = num >= 0 ? num / m : -((-num + m - 1) / m);
+    i0 = fl + 1;
+    const double scale = double(m) / double(den);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int d = (i0 + q) * m - I * den;
+      d = d < 0 ? -d : d;
+      w[q] = d < den ? scale * (1.0 - double(d) / double(den)) : 0.0;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (i0 + q < 0 || i0 + q > n - 1) w[q] = 0.0;
+}
+
+__device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+
+// Full weighting of the fine residual at coarse node (I,J,K), boundary coarse
+// nodes included (fine boundary values of the residual are zero).
 template <typename T>
 __device__ __forceinline__ double full_weight(const GridDev& gf, const GridDev& gc, const T* __restrict__ rf, int I,
                                               int J, int K) {
-  const int fi = 2 * I, fj = 2 * J, fk = gc.dim == 3 ? 2 * K : 0;
+  int ix0, iy0, iz0 = 0;
+  double wx[4], wy[4], wz[4] = {1.0, 0.0, 0.0, 0.0};
+  restrict_weights(I, gf.nx, gc.nx, map_mode(gf.nx, gc.nx), ix0, wx);
+  restrict_weights(J, gf.ny, gc.ny, map_mode(gf.ny, gc.ny), iy0, wy);
+  const bool is3 = gc.dim == 3;
+  if (is3) restrict_weights(K, gf.nz, gc.nz, map_mode(gf.nz, gc.nz), iz0, wz);
   double acc = 0.0;
-  const int dk0 = gc.dim == 3 ? -1 : 0, dk1 = gc.dim == 3 ? 1 : 0;
-  for (int dk = dk0; dk <= dk1; ++dk) {
-    const int kk = fk + dk;
-    if (kk < 0 || kk >= gf.nz) continue;
-    const double wk = gc.dim == 3 ? (dk == 0 ? 0.5 : 0.25) : 1.0;
-    for (int dj = -1; dj <= 1; ++dj) {
-      const int jj = fj + dj;
-      if (jj < 0 || jj >= gf.ny) continue;
-      const double wjk = wk * (dj == 0 ? 0.5 : 0.25);
-      const long long row = ((long long)kk * gf.ny + jj) * gf.nx;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (wz[c] == 0.0) continue;
+    const long long plane = (long long)clampi(iz0 + c, gf.nz - 1) * gf.ny;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (wy[b] == 0.0) continue;
+      const T* row = rf + (plane + clampi(iy0 + b, gf.ny - 1)) * gf.nx;
       double rs = 0.0;
-      if (fi - 1 >= 0) rs += 0.25 * double(rf[row + fi - 1]);
-      rs += 0.5 * double(rf[row + fi]);
-      if (fi + 1 < gf.nx) rs += 0.25 * double(rf[row + fi + 1]);
-      acc += wjk * rs;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (wx[a] != 0.0) rs += wx[a] * double(row[clampi(ix0 + a, gf.nx - 1)]);
+      acc += wz[c] * wy[b] * rs;
     }
   }
   return acc;
@@ -690,7 +761,7 @@ __device__ __forceinline__ double ext_value(const GridDev& gc, const TC* __restr
   return coef == 0.0 ? 0.0 : coef * double(xc[cidx(gc, I, J, K)]);
 }
 
-// Trilinear (bilinear in 2D) prolongation of the coarse correction, extended
+// Trilinear (bilinear in 2D) interpolation of the coarse correction, extended
 // to the coarse boundary through the closures, added to the fine interior.
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc, const TC* __restrict__ xc,
@@ -701,35 +772,65 @@ __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc
   int k0, k1;
   column_range(gf, k0, k1);
   if (!(i >= 1 && i <= gf.nx - 2 && j >= 1 && j <= gf.ny - 2)) return;
-  const int I0 = i >> 1, I1 = (i + 1) >> 1, J0 = j >> 1, J1 = (j + 1) >> 1;
+  int I0, J0;
+  double tx, ty;
+  coarse_pos(i, gf.nx, gc.nx, map_mode(gf.nx, gc.nx), I0, tx);
+  coarse_pos(j, gf.ny, gc.ny, map_mode(gf.ny, gc.ny), J0, ty);
+  const int I1 = tx != 0.0 ? I0 + 1 : I0, J1 = ty != 0.0 ? J0 + 1 : J0;
   const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
+  const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
   for (int k = k0; k < k1; ++k) {
-    const int K0 = gf.dim == 3 ? k >> 1 : 0, K1 = gf.dim == 3 ? (k + 1) >> 1 : 0;
-    double v;
+    int K0 = 0, K1 = 0;
+    double tz = 0.0;
+    if (gf.dim == 3) {
+      coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+      K1 = tz != 0.0 ? K0 + 1 : K0;
+    }
+    double c000, c100, c010, c110, c001, c101, c011, c111;
     if (!xy_edge && !(gf.dim == 3 && (K0 == 0 || K1 == gc.nz - 1))) {
       const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
       const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
-      v = 0.125 * (double(xc[a0 + r0 + I0]) + double(xc[a0 + r0 + I1]) + double(xc[a0 + r1 + I0]) +
-                   double(xc[a0 + r1 + I1]) + double(xc[a1 + r0 + I0]) + double(xc[a1 + r0 + I1]) +
-                   double(xc[a1 + r1 + I0]) + double(xc[a1 + r1 + I1]));
+      c000 = double(xc[a0 + r0 + I0]);
+      c100 = double(xc[a0 + r0 + I1]);
+      c010 = double(xc[a0 + r1 + I0]);
+      c110 = double(xc[a0 + r1 + I1]);
+      c001 = double(xc[a1 + r0 + I0]);
+      c101 = double(xc[a1 + r0 + I1]);
+      c011 = double(xc[a1 + r1 + I0]);
+      c111 = double(xc[a1 + r1 + I1]);
     } else {
-      v = 0.125 * (ext_value(gc, xc, I0, J0, K0) + ext_value(gc, xc, I1, J0, K0) + ext_value(gc, xc, I0, J1, K0) +
-                   ext_value(gc, xc, I1, J1, K0) + ext_value(gc, xc, I0, J0, K1) + ext_value(gc, xc, I1, J0, K1) +
-                   ext_value(gc, xc, I0, J1, K1) + ext_value(gc, xc, I1, J1, K1));
+      c000 = ext_value(gc, xc, I0, J0, K0);
+      c100 = ext_value(gc, xc, I1, J0, K0);
+      c010 = ext_value(gc, xc, I0, J1, K0);
+      c110 = ext_value(gc, xc, I1, J1, K0);
+      c001 = ext_value(gc, xc, I0, J0, K1);
+      c101 = ext_value(gc, xc, I1, J0, K1);
+      c011 = ext_value(gc, xc, I0, J1, K1);
+      c111 = ext_value(gc, xc, I1, J1, K1);
     }
+    const double x00 = (1.0 - tx) * c000 + tx * c100, x10 = (1.0 - tx) * c010 + tx * c110;
+    const double x01 = (1.0 - tx) * c001 + tx * c101, x11 = (1.0 - tx) * c011 + tx * c111;
+    const double y0 = (1.0 - ty) * x00 + ty * x10, y1 = (1.0 - ty) * x01 + ty * x11;
+    const double v = (1.0 - tz) * y0 + tz * y1;
     const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
     xf[id] = T(double(xf[id]) + v);
   }
 }
 
-// Coarse k by injection k_c(I,J,K) = k_f(2I,2J,2K).
+// Coarse k by injection from the nearest fine node (k_c(I) = k_f(2I) for odd n).
+__device__ __forceinline__ int nearest_fine(int I, int n, int nc) {
+  return (I * (n - 1) + (nc - 1) / 2) / (nc - 1);
+}
+
 template <typename KT>
 __global__ void k_inject(GridDev gf, GridDev gc, const KT* __restrict__ kf, KT* __restrict__ kc) {
   for (long long t = gtid(); t < gc.n; t += gstride()) {
     const int I = int(t % gc.nx);
     const int J = int((t / gc.nx) % gc.ny);
     const int K = int(t / gc.sxy);
-    kc[t] = kf[((long long)(gc.dim == 3 ? 2 * K : 0) * gf.ny + 2 * J) * gf.nx + 2 * I];
+    const int fi = nearest_fine(I, gf.nx, gc.nx), fj = nearest_fine(J, gf.ny, gc.ny);
+    const int fk = gc.dim == 3 ? nearest_fine(K, gf.nz, gc.nz) : 0;
+    kc[t] = kf[((long long)fk * gf.ny + fj) * gf.nx + fi];
   }
 }
 

@@ -187,12 +187,17 @@ void build_faces(Context* ctx, const pdeb200_problem* p, int nx, int ny, int nz,
     face_dims(f, nx, ny, nz, &w, &hgt);
     face_dims(f, fnx, fny, fnz, &fw, &fh);
     const int cnt = w * hgt;
+    // coarse face node -> nearest fine face node (stride 2^l for odd sizes)
+    auto nearest = [](int a, int wc, int wf) -> long long {
+      if (wc <= 1) return 0;
+      return ((long long)a * (wf - 1) + (wc - 1) / 2) / (wc - 1);
+    };
     auto sample = [&](const double* arr, std::vector<double>* out) {
       out->resize(cnt);
       for (int b = 0; b < hgt; ++b)
         for (int a = 0; a < w; ++a) {
-          long long fi = (long long)a * stride;
-          long long fj = (long long)b * stride;
+          long long fi = stride == 1 ? a : nearest(a, w, fw);
+          long long fj = stride == 1 ? b : nearest(b, hgt, fh);
           if (fi >= fw) fi = fw - 1;
           if (fj >= fh) fj = fh - 1;
           (*out)[(size_t)b * w + a] = arr[fj * fw + fi];

@@ -272,10 +272,31 @@ void folded_residual_report(Context* ctx, DevProblem& P, const Coef& cf, const d
 
 // ------------------------------------------------------------ MG hierarchy
 
-inline bool can_coarsen(const GridDev& g) {
-  if (!(g.nx >= 5 && (g.nx & 1) && g.ny >= 5 && (g.ny & 1))) return false;
-  if (g.dim == 3 && !(g.nz >= 5 && (g.nz & 1))) return false;
-  return true;
+// Coarsening of the B200 hierarchy, per dimension: a dimension with >= 5 nodes
+// coarsens to ceil((n-1)/2)+1 nodes (2:1 and nested for odd n) when its
+// spacing is below twice the smallest spacing of the grid; others keep their
+// size (semi-coarsening keeps the coarse cells near isotropic on elongated
+// domains). Returns false when no dimension coarsens.
+inline int coarse_size(int n) { return n / 2 + 1; }  // ceil((n-1)/2) + 1
+
+inline bool coarse_dims(const GridDev& g, const pdeb200_problem* hp, int nc[3]) {
+  const int n[3] = {g.nx, g.ny, g.nz};
+  const double len[3] = {hp->xmax - hp->xmin, hp->ymax - hp->ymin, hp->zmax - hp->zmin};
+  const int dims = g.dim == 3 ? 3 : 2;
+  double h[3], hmin = 0.0;
+  for (int d = 0; d < dims; ++d) {
+    h[d] = len[d] / double(n[d] - 1);
+    if (d == 0 || h[d] < hmin) hmin = h[d];
+  }
+  bool any = false;
+  for (int d = 0; d < 3; ++d) {
+    nc[d] = n[d];
+    if (d < dims && n[d] >= 5 && h[d] < 2.0 * hmin) {
+      nc[d] = coarse_size(n[d]);
+      any = true;
+    }
+  }
+  return any;
 }
 
 template <typename KT>
@@ -334,9 +355,10 @@ inline CoefNodal coarsen_coef(Context* ctx, const DevProblem&, const CoefNodal& 
   return c;
 }
 
-// Geometric hierarchy of the folded operator. Coarsening n_c = (n+1)/2 while
-// every active dimension is odd and >= 5 (down to 3 nodes in the smallest
-// dimension); face closures are rediscretised with the coarse spacing.
+// Geometric hierarchy of the folded operator. Coarsening per coarse_dims
+// (odd cubes nest 2:1 as in the reference's multigrid.cpp:150-170, continued
+// down to 3 nodes; even sizes use the non-nested maps of kernels.cuh); face
+// closures are rediscretised with the coarse spacing.
 // Each level has two field buffers: smoothing sweeps are fused red-black
 // passes that read one buffer and write the other.
 template <class Coef, typename T>
@@ -385,13 +407,14 @@ struct Hierarchy {
     l0.r = alloc(ctx, P.g.n);
     levels.push_back(l0);
     int stride = 1;
-    while ((int)levels.size() < max_levels && can_coarsen(levels.back().g)) {
+    int nc[3];
+    while ((int)levels.size() < max_levels && coarse_dims(levels.back().g, hp, nc)) {
       const GridDev& gf = levels.back().g;
       Level c;
       c.g = gf;
-      c.g.nx = (gf.nx + 1) / 2;
-      c.g.ny = (gf.ny + 1) / 2;
-      c.g.nz = gf.dim == 3 ? (gf.nz + 1) / 2 : 1;
+      c.g.nx = nc[0];
+      c.g.ny = nc[1];
+      c.g.nz = gf.dim == 3 ? nc[2] : 1;
       c.g.sxy = (long long)c.g.nx * c.g.ny;
       c.g.n = c.g.sxy * c.g.nz;
       stride *= 2;

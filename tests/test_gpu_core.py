@@ -137,6 +137,29 @@ def test_mgpcg_varcoef_3d(oracle_mod, n):
     assert rel_l2(got, ref) <= 1e-9
 
 
+@pytest.mark.parametrize("dims", [(34, 34, 34), (24, 19, 30), (129, 20, 17), (100, 37, 1), (258, 131, 1)])
+def test_mgpcg_uneven_sizes(oracle_mod, dims):
+    # even and mixed sizes: non-nested levels and semi-coarsening
+    nx, ny, nz = dims
+    rng = np.random.Generator(np.random.PCG64(sum(dims)))
+    p = GridProblem(nx, ny, nz, coef_kind=abi.COEF_DIVK)
+    p.k = np.exp(0.5 * rng.standard_normal(p.n))
+    p.f = rng.standard_normal(p.n)
+    if nz == 1:
+        p.faces = [FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(1.0),
+                   FaceBC(), FaceBC()]
+    else:
+        p.faces = [FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(1.0),
+                   FaceBC.neumann(0.1), FaceBC.dirichlet(0.0)]
+    opt = default_options(method=abi.MG_PCG, tol=1e-12, tol_mode=abi.TOL_RELATIVE, max_iter=300)
+    got, rep = solver.solve(p, opt)
+    st, ref, rrep = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rep.status == abi.OK
+    assert rrep.iterations <= 20
+    assert abs(rep.iterations - rrep.iterations) <= 1
+    assert rel_l2(got, ref) <= 1e-9
+
+
 def test_mgpcg_relative_1e10_true_residual(oracle_mod):
     p = synthetic.varcoef_poisson_3d(33, seed=8)
     opt = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=300)
