@@ -1786,6 +1786,8 @@ long rs_sizeof(int which) {
     case 4: return (long)sizeof(pdeb200_time_options);
     case 5: return (long)sizeof(pdeb200_projection_options);
     case 6: return (long)sizeof(pdeb200_projection_report);
+    case 7: return (long)sizeof(pdeb200_batch_options);
+    case 8: return (long)sizeof(pdeb200_batch_stats);
     default: return -1;
   }
 }

@@ -11,6 +11,7 @@
 #define ORACLE_RESTATE_H
 
 #include "pdeb200.h"
+#include "pdeb200_batch.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -1,4 +1,5 @@
-"""ctypes mirror of include/pdeb200.h and the loader for libpdeb200.so.
+"""ctypes mirror of include/pdeb200.h (and pdeb200_batch.h) and the loader
+for libpdeb200.so.
 
 The structures here must stay byte-identical to the C header; tests check
 their sizes against the library's own sizeof values (pdeb200_sizeof_*).
@@ -158,6 +159,47 @@ class KernelStat(C.Structure):
     ]
 
 
+class BatchOptions(C.Structure):
+    """pdeb200_batch_options (include/pdeb200_batch.h)."""
+    _fields_ = [
+        ("device", C.c_int32),
+        ("tile_x", C.c_int32),
+        ("tile_y", C.c_int32),
+        ("tile_z", C.c_int32),
+        ("pre_smooth", C.c_int32),
+        ("post_smooth", C.c_int32),
+        ("coarse_sweeps", C.c_int32),
+        ("max_inner", C.c_int32),
+        ("max_outer", C.c_int32),
+        ("bf16_coefficients", C.c_int32),
+        ("no_graph", C.c_int32),
+        ("autotune", C.c_int32),
+        ("inner_tol", C.c_double),
+        ("tune_cache", C.c_char_p),
+        ("stream", C.c_void_p),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class BatchStats(C.Structure):
+    """pdeb200_batch_stats (include/pdeb200_batch.h)."""
+    _fields_ = [
+        ("members", C.c_int32),
+        ("converged", C.c_int32),
+        ("cycles", C.c_int32),
+        ("max_levels", C.c_int32),
+        ("kernel_launches", C.c_int64),
+        ("tiles_level0", C.c_int64),
+        ("nodes", C.c_int64),
+        ("device_bytes", C.c_int64),
+        ("device_ms", C.c_double),
+        ("tune_ms", C.c_double),
+        ("tuned_from_cache", C.c_int32),
+        ("graph", C.c_int32),
+        ("reserved", C.c_int32 * 6),
+    ]
+
+
 FRAME_CB = C.CFUNCTYPE(C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -200,6 +242,25 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_jacobi_noalloc.restype = C.c_int32
     lib.pdeb200_jacobi_noalloc.argtypes = [P(Problem), C.c_int32, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
                                            P(Report)]
+    lib.pdeb200_batch_default_options.restype = None
+    lib.pdeb200_batch_default_options.argtypes = [P(BatchOptions)]
+    lib.pdeb200_batch_create.restype = C.c_int32
+    lib.pdeb200_batch_create.argtypes = [P(Problem), C.c_int32, P(BatchOptions), P(C.c_void_p), C.c_char_p,
+                                         C.c_size_t]
+    lib.pdeb200_batch_nodes.restype = C.c_int64
+    lib.pdeb200_batch_nodes.argtypes = [C.c_void_p]
+    lib.pdeb200_batch_offset.restype = C.c_int64
+    lib.pdeb200_batch_offset.argtypes = [C.c_void_p, C.c_int32]
+    lib.pdeb200_batch_load_rhs.restype = C.c_int32
+    lib.pdeb200_batch_load_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.pdeb200_batch_solve.restype = C.c_int32
+    lib.pdeb200_batch_solve.argtypes = [C.c_void_p, C.c_double, P(Report), P(BatchStats)]
+    lib.pdeb200_batch_read.restype = C.c_int32
+    lib.pdeb200_batch_read.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.pdeb200_batch_get_options.restype = C.c_int32
+    lib.pdeb200_batch_get_options.argtypes = [C.c_void_p, P(BatchOptions)]
+    lib.pdeb200_batch_destroy.restype = None
+    lib.pdeb200_batch_destroy.argtypes = [C.c_void_p]
     return lib
 
 

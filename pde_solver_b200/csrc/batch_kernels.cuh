@@ -1,0 +1,702 @@
+// Kernels of the batched solver. A batch is many independent grids ("members")
+// of mixed sizes and dimensions solved together: every phase of the solver is
+// ONE launch over a table of tiles that covers the matching level of every
+// member, so a 33x33 grid and a 129^3 grid share each launch and the small
+// grids no longer pay a launch per kernel.
+//
+// Per member the algorithm is FP32 MG-preconditioned CG inside FP64 iterative
+// refinement (the precision form): the outer residual r = b - A x, the
+// solution update, every inner product and the coarsest-grid solve are FP64;
+// the MG V-cycle and the inner Krylov vectors are FP32 (hierarchy k in FP32 or
+// BF16). Each member carries its own state machine (BMember::state) advanced
+// by the reductions' post steps, so members converge independently and a
+// finished member's tiles return at once.
+//
+// Tiles cover interior nodes only: node (i,j,k) of tile T is
+// i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w, k in [T.z0, T.z1).
+// A member's coarsest level is one whole-grid tile (coarse = 1), solved by
+// the block that restricts into it.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace pdeb {
+
+enum BState : int { kBDone = 0, kBNeedOuter = 1, kBInnerStart = 2, kBInnerRun = 3 };
+
+// One level of one member.
+struct BLevel {
+  GridDev g;
+  int kind;       // kConst / kDivk
+  int member;
+  int prev;       // finer level record (-1 on level 0)
+  int next;       // coarser level record (-1 on the coarsest)
+  int coarsest;
+  int level;
+  CoefConst cc;                                   // kConst stencil of this level
+  double ihx2, ihy2, ihz2, cx, dyc, dzc, e;       // kDivk scalars of this level
+  const void* kh;                                 // hierarchy k (float or bf16)
+  float* x;                                       // correction (level 0: z = M r)
+  float* b;                                       // right-hand side (level 0: PCG residual r)
+  float* r;                                       // residual scratch
+};
+
+// Per-member solver state and level-0 vectors.
+struct BMember {
+  int state;
+  int outer;        // outer residual evaluations so far
+  int inner;        // inner iterations of the current refinement step
+  int inner_total;
+  int max_inner, max_outer;
+  int tile0, ntiles;  // level-0 tiles [tile0, tile0 + ntiles)
+  int first;          // the coming p update starts a new inner solve
+  int status;
+  int e_valid;        // e holds a correction not yet added to x
+  int level0;
+  unsigned ticket;
+  int pad;
+  double bb;        // |b|^2 (FP64)
+  double rr0;       // |r|^2 at the start of the inner solve
+  double rr;        // inner |r|^2
+  double rr_outer;  // FP64 |b - A x|^2 at the last outer evaluation
+  double rz, alpha, beta;
+  double tol2;        // tol^2 (outer, relative to |b|)
+  double tol2_inner;  // inner_tol^2 (relative to rr0)
+  double* x64;
+  double* b64;
+  const double* f64;
+  const double* k64;
+  const float* k32;
+  float* p;
+  float* q;
+  float* e;
+};
+
+struct BTile {
+  int lev, member;
+  int x0, y0, w, h;
+  int z0, z1;
+  int coarse;
+  int pad;
+};
+
+// Copies a descriptor into shared memory (all threads; caller syncs).
+template <class S>
+__device__ __forceinline__ void bstage(S& dst, const S* src) {
+  static_assert(sizeof(S) % 4 == 0, "descriptor size");
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (int t = threadIdx.x; t < (int)(sizeof(S) / 4); t += blockDim.x) d[t] = __ldg(s + t);
+}
+
+__device__ __forceinline__ int bstate(const BMember* m) { return *((volatile const int*)&m->state); }
+__device__ __forceinline__ bool vcycle_state(int s) { return s == kBInnerStart || s == kBInnerRun; }
+
+// Folded stencil of interior node (i,j,kk) of level L with coefficient field k.
+template <typename T, typename KT>
+__device__ __forceinline__ Stencil<T> bstencil(const BLevel& L, const KT* k, int i, int j, int kk, long long id,
+                                               double* shift) {
+  Stencil<T> s;
+  if (L.kind == kConst) {
+    s = L.cc.template at<T>(L.g, id);
+  } else {
+    CoefDivk<KT> c;
+    c.k = k;
+    c.ihx2 = L.ihx2;
+    c.ihy2 = L.ihy2;
+    c.ihz2 = L.ihz2;
+    c.cx = L.cx;
+    c.dyc = L.dyc;
+    c.dzc = L.dzc;
+    c.e = L.e;
+    s = c.template at<T>(L.g, id);
+  }
+  fold_faces<T>(L.g, i, j, kk, s, shift);
+  return s;
+}
+
+__device__ __forceinline__ long long bid(const GridDev& g, int i, int j, int k) {
+  return ((long long)k * g.ny + j) * g.nx + i;
+}
+
+// Per-member reduction: every tile stores its block sum, the member's last
+// tile (atomic ticket) adds the member's partials in tile order and runs
+// post(member, sums). Deterministic for a given tiling, and independent of
+// which other members share the launch.
+template <int NV, class Post>
+__device__ __forceinline__ void member_reduce(double (&v)[NV], double* partials, BMember* m, int tile,
+                                              const Post& post) {
+  block_sum<NV>(v);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) partials[(size_t)tile * NV + q] = v[q];
+    __threadfence();
+    const unsigned t = atomicAdd(&m->ticket, 1u);
+    last = (t == (unsigned)m->ntiles - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+  for (int b = threadIdx.x; b < m->ntiles; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += __ldcg(partials + (size_t)(m->tile0 + b) * NV + q);
+  block_sum<NV>(acc);
+  if (threadIdx.x == 0) {
+    post(m, acc);
+    m->ticket = 0u;
+  }
+}
+
+// ------------------------------------------------------------------ posts
+
+struct BPostOuter {
+  int* active;
+  __device__ void operator()(BMember* m, const double* v) const {
+    const double rr = v[0];
+    if (m->outer == 0) m->bb = rr;  // x = 0: r = b
+    m->rr_outer = rr;
+    m->outer += 1;
+    m->e_valid = 0;
+    int done = -1;
+    if (!(rr == rr) || rr > 1.7e308) done = PDEB200_ERR_BREAKDOWN;
+    else if (m->bb == 0.0 || rr <= m->tol2 * m->bb) done = PDEB200_OK;
+    else if (m->outer > m->max_outer) done = PDEB200_ERR_NOT_CONVERGED;
+    if (done >= 0) {
+      m->status = done;
+      m->state = kBDone;
+      atomicSub(active, 1);
+    } else {
+      m->state = kBInnerStart;
+      m->inner = 0;
+      m->rr0 = rr;
+      m->rr = rr;
+    }
+  }
+};
+
+struct BPostPQ {
+  __device__ void operator()(BMember* m, const double* v) const {
+    const double pq = v[0];
+    if (pq > 0.0 && pq < 1.7e308 && m->rz > 0.0) {
+      m->alpha = m->rz / pq;
+    } else {
+      m->state = kBNeedOuter;  // breakdown: restart from the current refinement
+    }
+  }
+};
+
+struct BPostUpdate {
+  __device__ void operator()(BMember* m, const double* v) const {
+    const double rr = v[0];
+    m->inner += 1;
+    m->inner_total += 1;
+    m->rr = rr;
+    if (!(rr == rr) || rr > 1.7e308) {
+      m->e_valid = 0;
+      m->state = kBNeedOuter;
+      return;
+    }
+    m->e_valid = 1;
+    if (rr <= m->tol2_inner * m->rr0 || m->inner >= m->max_inner) m->state = kBNeedOuter;
+  }
+};
+
+struct BPostRZ {
+  __device__ void operator()(BMember* m, const double* v) const {
+    const double rz = v[0];
+    if (!(rz > 0.0) || rz > 1.7e308) {
+      m->state = kBNeedOuter;
+      return;
+    }
+    if (m->state == kBInnerStart) {
+      m->first = 1;
+      m->beta = 0.0;
+      m->state = kBInnerRun;
+    } else {
+      m->first = 0;
+      m->beta = rz / m->rz;
+    }
+    m->rz = rz;
+  }
+};
+
+// --------------------------------------------------------------- kernels
+
+constexpr int kBThreads = 256;
+
+// Folded right-hand side b64 = -f - (face shift) and x64 = 0 on level 0.
+__global__ void __launch_bounds__(kBThreads) kb_rhs(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                    const BMember* __restrict__ mem) {
+  const BTile T = tiles[blockIdx.x];
+  __shared__ BLevel L;
+  bstage(L, lv + T.lev);
+  __syncthreads();
+  const BMember& m = mem[T.member];
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    for (int kk = T.z0; kk < T.z1; ++kk) {
+      const long long id = bid(L.g, i, j, kk);
+      double sh = 0.0;
+      (void)bstencil<double, double>(L, m.k64, i, j, kk, id, &sh);
+      m.b64[id] = -(m.f64 ? m.f64[id] : 0.0) - sh;
+      m.x64[id] = 0.0;
+    }
+  }
+}
+
+// x64 += e for members about to take an outer step with a pending correction.
+__global__ void __launch_bounds__(kBThreads) kb_xupdate(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                        const BMember* __restrict__ mem) {
+  const BTile T = tiles[blockIdx.x];
+  const BMember* m = mem + T.member;
+  if (bstate(m) != kBNeedOuter || !*((volatile const int*)&m->e_valid)) return;
+  const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
+  double* x = m->x64;
+  const float* e = m->e;
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    for (int kk = T.z0; kk < T.z1; ++kk) {
+      const long long id = ((long long)kk * ny + j) * nx + i;
+      x[id] += double(e[id]);
+    }
+  }
+}
+
+// Outer FP64 residual r = b - A x; the FP32 copy is the inner right-hand side.
+__global__ void __launch_bounds__(kBThreads) kb_outer(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                      BMember* mem, double* partials, int* active) {
+  const BTile T = tiles[blockIdx.x];
+  BMember* m = mem + T.member;
+  if (bstate(m) != kBNeedOuter) return;
+  __shared__ BLevel L;
+  bstage(L, lv + T.lev);
+  __syncthreads();
+  const double* __restrict__ x = m->x64;
+  const double* __restrict__ b = m->b64;
+  float* __restrict__ r32 = L.b;
+  const double* k64 = m->k64;
+  double acc[1] = {0.0};
+  const int cols = T.w * T.h;
+  const int nx = L.g.nx;
+  const long long sxy = L.g.sxy;
+  const bool is3 = L.g.dim == 3;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    long long id = bid(L.g, i, j, T.z0);
+    double zm = is3 ? x[id - sxy] : 0.0;
+    double zc = x[id];
+    for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
+      const double zp = is3 ? x[id + sxy] : 0.0;
+      const Stencil<double> s = bstencil<double, double>(L, k64, i, j, kk, id, nullptr);
+      const double v = b[id] - (s.c * zc + nb_sum<double>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm,
+                                                           L.g.dim));
+      r32[id] = float(v);
+      acc[0] += v * v;
+      zm = zc;
+      zc = zp;
+    }
+  }
+  member_reduce<1>(acc, partials, m, blockIdx.x, BPostOuter{active});
+}
+
+// q = A p (FP32 operator, FP32 k), sum p.q in FP64.
+__global__ void __launch_bounds__(kBThreads) kb_apply_pq(const BTile* __restrict__ tiles,
+                                                         const BLevel* __restrict__ lv, BMember* mem,
+                                                         double* partials) {
+  const BTile T = tiles[blockIdx.x];
+  BMember* m = mem + T.member;
+  if (bstate(m) != kBInnerRun) return;
+  __shared__ BLevel L;
+  bstage(L, lv + T.lev);
+  __syncthreads();
+  const float* __restrict__ p = m->p;
+  float* __restrict__ q = m->q;
+  const float* k32 = m->k32;
+  double acc[1] = {0.0};
+  const int cols = T.w * T.h;
+  const int nx = L.g.nx;
+  const long long sxy = L.g.sxy;
+  const bool is3 = L.g.dim == 3;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    long long id = bid(L.g, i, j, T.z0);
+    float zm = is3 ? p[id - sxy] : 0.f;
+    float zc = p[id];
+    for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
+      const float zp = is3 ? p[id + sxy] : 0.f;
+      const Stencil<float> s = bstencil<float, float>(L, k32, i, j, kk, id, nullptr);
+      const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, L.g.dim);
+      q[id] = v;
+      acc[0] += double(zc) * double(v);
+      zm = zc;
+      zc = zp;
+    }
+  }
+  member_reduce<1>(acc, partials, m, blockIdx.x, BPostPQ{});
+}
+
+// e (+)= alpha p, r -= alpha q, sum r.r in FP64.
+__global__ void __launch_bounds__(kBThreads) kb_update(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                       BMember* mem, double* partials) {
+  const BTile T = tiles[blockIdx.x];
+  BMember* m = mem + T.member;
+  if (bstate(m) != kBInnerRun) return;
+  const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
+  float* __restrict__ r = lv[T.lev].b;
+  const float* __restrict__ p = m->p;
+  const float* __restrict__ q = m->q;
+  float* __restrict__ e = m->e;
+  const float a = float(*((volatile const double*)&m->alpha));
+  const bool first = *((volatile const int*)&m->inner) == 0;
+  double acc[1] = {0.0};
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    for (int kk = T.z0; kk < T.z1; ++kk) {
+      const long long id = ((long long)kk * ny + j) * nx + i;
+      e[id] = first ? a * p[id] : e[id] + a * p[id];
+      const float rv = r[id] - a * q[id];
+      r[id] = rv;
+      acc[0] += double(rv) * double(rv);
+    }
+  }
+  member_reduce<1>(acc, partials, m, blockIdx.x, BPostUpdate{});
+}
+
+// sum r.z in FP64 (starts a new inner solve or gives beta).
+__global__ void __launch_bounds__(kBThreads) kb_rz(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                   BMember* mem, double* partials) {
+  const BTile T = tiles[blockIdx.x];
+  BMember* m = mem + T.member;
+  if (!vcycle_state(bstate(m))) return;
+  const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
+  const float* __restrict__ r = lv[T.lev].b;
+  const float* __restrict__ z = lv[T.lev].x;
+  double acc[1] = {0.0};
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    for (int kk = T.z0; kk < T.z1; ++kk) {
+      const long long id = ((long long)kk * ny + j) * nx + i;
+      acc[0] += double(r[id]) * double(z[id]);
+    }
+  }
+  member_reduce<1>(acc, partials, m, blockIdx.x, BPostRZ{});
+}
+
+// p = z + beta p (p = z when the inner solve starts).
+__global__ void __launch_bounds__(kBThreads) kb_pupdate(const BTile* __restrict__ tiles,
+                                                        const BLevel* __restrict__ lv, const BMember* mem) {
+  const BTile T = tiles[blockIdx.x];
+  const BMember* m = mem + T.member;
+  if (bstate(m) != kBInnerRun) return;
+  const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
+  const float* __restrict__ z = lv[T.lev].x;
+  float* __restrict__ p = m->p;
+  const bool first = *((volatile const int*)&m->first) != 0;
+  const float bt = float(*((volatile const double*)&m->beta));
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    for (int kk = T.z0; kk < T.z1; ++kk) {
+      const long long id = ((long long)kk * ny + j) * nx + i;
+      p[id] = first ? z[id] : z[id] + bt * p[id];
+    }
+  }
+}
+
+// One red-black colour pass of the V-cycle smoother on level tiles. from_zero:
+// x is taken as zero (first pass of a level): the colour's nodes get b/diag,
+// the other colour's nodes 0.
+template <typename KT>
+__global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                       const BMember* mem, int color, int from_zero) {
+  const BTile T = tiles[blockIdx.x];
+  if (T.coarse) return;
+  if (!vcycle_state(bstate(mem + T.member))) return;
+  __shared__ BLevel L;
+  bstage(L, lv + T.lev);
+  __syncthreads();
+  const KT* k = static_cast<const KT*>(L.kh);
+  float* __restrict__ x = L.x;
+  const float* __restrict__ b = L.b;
+  const int nx = L.g.nx;
+  const long long sxy = L.g.sxy;
+  const bool is3 = L.g.dim == 3;
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    if (from_zero) {
+      for (int kk = T.z0; kk < T.z1; ++kk) {
+        const long long id = bid(L.g, i, j, kk);
+        if (((i + j + kk) & 1) == color) {
+          const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+          x[id] = b[id] / s.c;
+        } else {
+          x[id] = 0.f;
+        }
+      }
+    } else {
+      for (int kk = T.z0 + ((i + j + T.z0 + color) & 1); kk < T.z1; kk += 2) {
+        const long long id = bid(L.g, i, j, kk);
+        const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+        const float zp = is3 ? x[id + sxy] : 0.f;
+        const float zm = is3 ? x[id - sxy] : 0.f;
+        x[id] = (b[id] - nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, L.g.dim)) / s.c;
+      }
+    }
+  }
+}
+
+// Level residual r = b - A x on level tiles.
+template <typename KT>
+__global__ void __launch_bounds__(kBThreads) kb_residual(const BTile* __restrict__ tiles,
+                                                         const BLevel* __restrict__ lv, const BMember* mem) {
+  const BTile T = tiles[blockIdx.x];
+  if (T.coarse) return;
+  if (!vcycle_state(bstate(mem + T.member))) return;
+  __shared__ BLevel L;
+  bstage(L, lv + T.lev);
+  __syncthreads();
+  const KT* k = static_cast<const KT*>(L.kh);
+  const float* __restrict__ x = L.x;
+  const float* __restrict__ b = L.b;
+  float* __restrict__ r = L.r;
+  const int nx = L.g.nx;
+  const long long sxy = L.g.sxy;
+  const bool is3 = L.g.dim == 3;
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    long long id = bid(L.g, i, j, T.z0);
+    float zm = is3 ? x[id - sxy] : 0.f;
+    float zc = x[id];
+    for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
+      const float zp = is3 ? x[id + sxy] : 0.f;
+      const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+      r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, L.g.dim));
+      zm = zc;
+      zc = zp;
+    }
+  }
+}
+
+// Coarsest-level solve inside one block: `sweeps` red-black sweeps from zero
+// in FP64 (shared memory when the grid has at most kBCoarseSmem nodes, else
+// in place on the FP32 field with FP64 arithmetic).
+constexpr int kBCoarseSmem = 256;
+
+template <typename KT>
+__device__ void bcoarse_solve(const BLevel& C, int sweeps) {
+  __shared__ double cs[kBCoarseSmem];
+  const KT* k = static_cast<const KT*>(C.kh);
+  const GridDev& g = C.g;
+  const int kb = g.dim == 3 ? 1 : 0, ke = g.dim == 3 ? g.nz - 1 : 1;
+  const int ni = g.nx - 2, nj = g.ny - 2, nk = ke - kb;
+  const int total = ni * nj * nk;
+  const bool smem = g.n <= kBCoarseSmem;
+  if (smem) {
+    for (int t = threadIdx.x; t < (int)g.n; t += blockDim.x) cs[t] = 0.0;
+  } else {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int i = 1 + t % ni, j = 1 + (t / ni) % nj, kk = kb + t / (ni * nj);
+      C.x[bid(g, i, j, kk)] = 0.f;
+    }
+  }
+  __syncthreads();
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int i = 1 + t % ni, j = 1 + (t / ni) % nj, kk = kb + t / (ni * nj);
+        if (((i + j + kk) & 1) != color) continue;
+        const long long id = bid(g, i, j, kk);
+        const Stencil<double> st = bstencil<double, KT>(C, k, i, j, kk, id, nullptr);
+        double v;
+        if (smem) {
+          const int q = (int)id, nx = g.nx, sxy = (int)g.sxy;
+          v = st.xp * cs[q + 1] + st.xm * cs[q - 1] + st.yp * cs[q + nx] + st.ym * cs[q - nx];
+          if (g.dim == 3) v += st.zp * cs[q + sxy] + st.zm * cs[q - sxy];
+          cs[q] = (double(C.b[id]) - v) / st.c;
+        } else {
+          const float* x = C.x;
+          v = st.xp * double(x[id + 1]) + st.xm * double(x[id - 1]) + st.yp * double(x[id + g.nx]) +
+              st.ym * double(x[id - g.nx]);
+          if (g.dim == 3) v += st.zp * double(x[id + g.sxy]) + st.zm * double(x[id - g.sxy]);
+          C.x[id] = float((double(C.b[id]) - v) / st.c);
+        }
+      }
+      __syncthreads();
+    }
+  if (smem)
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int i = 1 + t % ni, j = 1 + (t / ni) % nj, kk = kb + t / (ni * nj);
+      const long long id = bid(g, i, j, kk);
+      C.x[id] = float(cs[id]);
+    }
+}
+
+// Restriction into level-(l+1) tiles: coarse b = Ext^T P^T r_fine at interior
+// coarse nodes (the boundary-closure fold recomputes the full weight of each
+// Neumann/Robin boundary node that feeds an interior one). A whole-grid tile
+// of a coarsest level then solves that level in the same block.
+template <typename KT>
+__global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict__ tiles,
+                                                         const BLevel* __restrict__ lv, const BMember* mem,
+                                                         int coarse_sweeps) {
+  const BTile T = tiles[blockIdx.x];
+  if (!vcycle_state(bstate(mem + T.member))) return;
+  __shared__ BLevel C;
+  __shared__ BLevel F;
+  bstage(C, lv + T.lev);
+  __syncthreads();
+  bstage(F, lv + C.prev);
+  __syncthreads();
+  const GridDev& gc = C.g;
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int I = 1 + T.x0 + t % T.w, J = 1 + T.y0 + t / T.w;
+    const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
+    const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
+    for (int K = T.z0; K < T.z1; ++K) {
+      double acc = full_weight<float>(F.g, gc, F.r, I, J, K);
+      const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+      if (dxl | dxh | dyl | dyh | dzl | dzh) {
+        for (int dk = dzl; dk <= dzh; ++dk)
+          for (int dj = dyl; dj <= dyh; ++dj)
+            for (int di = dxl; di <= dxh; ++di) {
+              if (di == 0 && dj == 0 && dk == 0) continue;
+              int ci = I + di, cj = J + dj, ck = K + dk;
+              const double coef = ext_chain(gc, ci, cj, ck);
+              if (coef != 0.0 && ci == I && cj == J && ck == K)
+                acc += coef * full_weight<float>(F.g, gc, F.r, I + di, J + dj, K + dk);
+            }
+      }
+      C.b[bid(gc, I, J, K)] = float(acc);
+    }
+  }
+  if (T.coarse) {
+    __syncthreads();
+    bcoarse_solve<KT>(C, coarse_sweeps);
+  }
+}
+
+// x_l += P Ext(x_{l+1}) on level-l tiles of members with a coarser level.
+__global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+                                                        const BMember* mem) {
+  const BTile T = tiles[blockIdx.x];
+  if (T.coarse) return;
+  if (!vcycle_state(bstate(mem + T.member))) return;
+  __shared__ BLevel F;
+  __shared__ BLevel C;
+  bstage(F, lv + T.lev);
+  __syncthreads();
+  bstage(C, lv + F.next);
+  __syncthreads();
+  const GridDev& gf = F.g;
+  const GridDev& gc = C.g;
+  const float* __restrict__ xc = C.x;
+  float* __restrict__ xf = F.x;
+  const int xmode = map_mode(gf.nx, gc.nx), ymode = map_mode(gf.ny, gc.ny);
+  const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
+  const int cols = T.w * T.h;
+  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
+    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+    int I0, J0;
+    double tx, ty;
+    coarse_pos(i, gf.nx, gc.nx, xmode, I0, tx);
+    coarse_pos(j, gf.ny, gc.ny, ymode, J0, ty);
+    const int I1 = tx != 0.0 ? I0 + 1 : I0, J1 = ty != 0.0 ? J0 + 1 : J0;
+    const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
+    for (int k = T.z0; k < T.z1; ++k) {
+      int K0 = 0, K1 = 0;
+      double tz = 0.0;
+      if (gf.dim == 3) {
+        coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+        K1 = tz != 0.0 ? K0 + 1 : K0;
+      }
+      double c000, c100, c010, c110, c001, c101, c011, c111;
+      if (!xy_edge && !(gf.dim == 3 && (K0 == 0 || K1 == gc.nz - 1))) {
+        const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
+        const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
+        c000 = double(xc[a0 + r0 + I0]);
+        c100 = double(xc[a0 + r0 + I1]);
+        c010 = double(xc[a0 + r1 + I0]);
+        c110 = double(xc[a0 + r1 + I1]);
+        c001 = double(xc[a1 + r0 + I0]);
+        c101 = double(xc[a1 + r0 + I1]);
+        c011 = double(xc[a1 + r1 + I0]);
+        c111 = double(xc[a1 + r1 + I1]);
+      } else {
+        c000 = ext_value(gc, xc, I0, J0, K0);
+        c100 = ext_value(gc, xc, I1, J0, K0);
+        c010 = ext_value(gc, xc, I0, J1, K0);
+        c110 = ext_value(gc, xc, I1, J1, K0);
+        c001 = ext_value(gc, xc, I0, J0, K1);
+        c101 = ext_value(gc, xc, I1, J0, K1);
+        c011 = ext_value(gc, xc, I0, J1, K1);
+        c111 = ext_value(gc, xc, I1, J1, K1);
+      }
+      const double x00 = (1.0 - tx) * c000 + tx * c100, x10 = (1.0 - tx) * c010 + tx * c110;
+      const double x01 = (1.0 - tx) * c001 + tx * c101, x11 = (1.0 - tx) * c011 + tx * c111;
+      const double y0 = (1.0 - ty) * x00 + ty * x10, y1 = (1.0 - ty) * x01 + ty * x11;
+      const double v = (1.0 - tz) * y0 + tz * y1;
+      const long long id = bid(gf, i, j, k);
+      xf[id] = float(double(xf[id]) + v);
+    }
+  }
+}
+
+// Boundary nodes of each member's FP64 solution from the closures (reference
+// phase order, Dirichlet last); one block per member.
+__global__ void __launch_bounds__(kBThreads) kb_fill_boundary(const BLevel* __restrict__ lv,
+                                                              const BMember* __restrict__ mem) {
+  const BMember* m = mem + blockIdx.x;
+  __shared__ BLevel L;
+  bstage(L, lv + m->level0);
+  __syncthreads();
+  const GridDev& g = L.g;
+  double* u = m->x64;
+  const long long nyz = (long long)g.ny * g.nz, nxz = (long long)g.nx * g.nz, nxy = (long long)g.nx * g.ny;
+  const long long total = 2 * nyz + 2 * nxz + (g.dim == 3 ? 2 * nxy : 0);
+  // one thread per face node; a node shared by faces is written by the first
+  // face (in face order) that contains it
+  for (long long t = threadIdx.x; t < total; t += blockDim.x) {
+    int i, j, k, f;
+    long long q = t;
+    if (q < 2 * nyz) {
+      f = q < nyz ? kLeft : kRight;
+      i = q < nyz ? 0 : g.nx - 1;
+      q %= nyz;
+      j = int(q % g.ny);
+      k = int(q / g.ny);
+    } else if ((q -= 2 * nyz) < 2 * nxz) {
+      f = q < nxz ? kBottom : kTop;
+      j = q < nxz ? 0 : g.ny - 1;
+      q %= nxz;
+      i = int(q % g.nx);
+      k = int(q / g.nx);
+    } else {
+      q -= 2 * nxz;
+      f = q < nxy ? kFront : kBack;
+      k = q < nxy ? 0 : g.nz - 1;
+      q %= nxy;
+      i = int(q % g.nx);
+      j = int(q / g.nx);
+    }
+    const bool on[6] = {i == 0, i == g.nx - 1, j == 0, j == g.ny - 1, g.dim == 3 && k == 0,
+                        g.dim == 3 && k == g.nz - 1};
+    int owner = -1;
+    for (int w = 0; w < 6 && owner < 0; ++w)
+      if (on[w]) owner = w;
+    if (owner != f) continue;
+    u[bid(g, i, j, k)] = boundary_final(g, u, i, j, k, true);
+  }
+}
+
+}  // namespace pdeb

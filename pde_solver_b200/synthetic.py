@@ -78,3 +78,30 @@ def varcoef_poisson_2d(n: int, seed: int, sigma: float = 0.5) -> GridProblem:
     p.k = lognormal_k((n, n), sigma, seed).reshape(-1)
     p.f = gaussian((n, n), seed + 1).reshape(-1)
     return p
+
+
+def batch_sides(n2d: int, n3d: int, seed: int, lo2=33, hi2=513, lo3=17, hi3=129):
+    """Sides of the batched workload: 2D sides round(exp(U[ln lo2, ln hi2])),
+    3D sides round(exp(U[ln lo3, ln hi3]))."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s2 = np.rint(np.exp(rng.uniform(np.log(lo2), np.log(hi2), n2d))).astype(int)
+    s3 = np.rint(np.exp(rng.uniform(np.log(lo3), np.log(hi3), n3d))).astype(int)
+    return s2, s3
+
+
+def batch_members(n2d: int = 2048, n3d: int = 256, seed: int = 4242, sigma: float = 0.5,
+                  lo2=33, hi2=513, lo3=17, hi3=129) -> list:
+    """Independent Poisson/diffusion grids -div(k grad u) = F with k = exp(sigma g)
+    (g iid N(0,1) per node, no smoothing), F ~ N(0,1), Dirichlet 0, each seeded
+    by its index: n2d square 2D grids then n3d cubic 3D grids."""
+    s2, s3 = batch_sides(n2d, n3d, seed, lo2, hi2, lo3, hi3)
+    out = []
+    for q, n in enumerate(list(s2) + list(s3)):
+        rng = np.random.Generator(np.random.PCG64([seed, q]))
+        is3 = q >= n2d
+        shape = (n, n, n) if is3 else (n, n)
+        p = GridProblem(n, n, n if is3 else 1, coef_kind=abi.COEF_DIVK)
+        p.k = np.exp(sigma * rng.standard_normal(shape)).reshape(-1)
+        p.f = (-rng.standard_normal(shape)).reshape(-1)
+        out.append(p)
+    return out

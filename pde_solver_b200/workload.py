@@ -1,8 +1,10 @@
 """Run the benchmark workloads through the C ABI without timing harness:
 
     python -m pde_solver_b200.workload --n 257 --solves 2 [--method MG_PCG] [--mixed]
+    python -m pde_solver_b200.workload --batch 2048,256 --solves 2
 
-Used as the target of profiler runs (each solve is the step `bench.py` times).
+Used as the target of profiler runs (each solve is the step `bench.py` times;
+--batch runs the batched workload: n2d 2D grids and n3d 3D grids).
 """
 from __future__ import annotations
 
@@ -20,7 +22,22 @@ def main(argv=None) -> int:
     ap.add_argument("--method", default="MG_PCG", choices=["MG_PCG", "MG_BICGSTAB", "CG", "JACOBI"])
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--workload", default="varcoef3d", choices=["varcoef3d", "convdiff3d"])
+    ap.add_argument("--batch", default="", help="n2d,n3d: batched workload instead of one grid")
+    ap.add_argument("--bf16", action="store_true")
     a = ap.parse_args(argv)
+    if a.batch:
+        from .batch import Batch
+
+        n2d, n3d = (int(v) for v in a.batch.split(","))
+        ms = synthetic.batch_members(n2d, n3d)
+        b = Batch(ms, bf16_coefficients=1 if a.bf16 else 0)
+        for _ in range(a.solves):
+            b.solve(1e-10)
+            s = b.stats
+            print(f"members={s.members} converged={s.converged} cycles={s.cycles} device_ms={s.device_ms:.2f} "
+                  f"launches={s.kernel_launches}", flush=True)
+        b.close()
+        return 0
     if a.workload == "varcoef3d":
         p = synthetic.varcoef_poisson_3d(a.n, seed=1234)
     else:

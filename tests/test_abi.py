@@ -1,5 +1,5 @@
 """CPU checks of the C-ABI boundary: the library loads, exports every entry
-point include/pdeb200.h declares, and the ctypes mirror matches the C layout."""
+point include/*.h declares, and the ctypes mirror matches the C layout."""
 import ctypes as C
 import os
 import re
@@ -12,7 +12,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "pdeb200.h")).read()
+    inc = os.path.join(ROOT, "include")
+    text = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(pdeb200_[a-z0-9_]+)\s*\(", text)) - {"pdeb200_frame_cb"})
 
@@ -29,7 +30,8 @@ def test_abi_version(lib):
 
 
 @pytest.mark.parametrize("which,cls", [(0, abi.Face), (1, abi.Problem), (2, abi.Options), (3, abi.Report),
-                                       (4, abi.TimeOptions), (5, abi.ProjectionOptions), (6, abi.ProjectionReport)])
+                                       (4, abi.TimeOptions), (5, abi.ProjectionOptions), (6, abi.ProjectionReport),
+                                       (7, abi.BatchOptions), (8, abi.BatchStats)])
 def test_struct_layout_matches_header(oracle_mod, which, cls):
     assert oracle_mod.restate().rs_sizeof(which) == C.sizeof(cls)
 
