@@ -1788,6 +1788,10 @@ long rs_sizeof(int which) {
     case 6: return (long)sizeof(pdeb200_projection_report);
     case 7: return (long)sizeof(pdeb200_batch_options);
     case 8: return (long)sizeof(pdeb200_batch_stats);
+    case 9: return (long)sizeof(pdeb200_server_options);
+    case 10: return (long)sizeof(pdeb200_request);
+    case 11: return (long)sizeof(pdeb200_result);
+    case 12: return (long)sizeof(pdeb200_server_stats);
     default: return -1;
   }
 }

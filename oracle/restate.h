@@ -12,6 +12,7 @@
 
 #include "pdeb200.h"
 #include "pdeb200_batch.h"
+#include "pdeb200_server.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -1,5 +1,5 @@
-"""ctypes mirror of include/pdeb200.h (and pdeb200_batch.h) and the loader
-for libpdeb200.so.
+"""ctypes mirror of include/pdeb200.h (and pdeb200_batch.h, pdeb200_server.h)
+and the loader for libpdeb200.so.
 
 The structures here must stay byte-identical to the C header; tests check
 their sizes against the library's own sizeof values (pdeb200_sizeof_*).
@@ -200,6 +200,89 @@ class BatchStats(C.Structure):
     ]
 
 
+REQ_POISSON, REQ_HEAT, REQ_PROJECTION = 0, 1, 2
+
+
+class ServerOptions(C.Structure):
+    """pdeb200_server_options (include/pdeb200_server.h)."""
+    _fields_ = [
+        ("device", C.c_int32),
+        ("lanes", C.c_int32),
+        ("max_batch", C.c_int32),
+        ("precision", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("queue_capacity", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("batch", BatchOptions),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class Request(C.Structure):
+    """pdeb200_request (include/pdeb200_server.h)."""
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("steps", C.c_int32),
+        ("problem", C.POINTER(Problem)),
+        ("tol", C.c_double),
+        ("t_start", C.c_double),
+        ("dt", C.c_double),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("max_iter", C.c_int32),
+        ("dx", C.c_double),
+        ("dy", C.c_double),
+        ("dz", C.c_double),
+        ("proj_dt", C.c_double),
+        ("proj_tol", C.c_double),
+        ("u", C.POINTER(C.c_double)),
+        ("v", C.POINTER(C.c_double)),
+        ("w", C.POINTER(C.c_double)),
+        ("p", C.POINTER(C.c_double)),
+        ("out", C.POINTER(C.c_double)),
+    ]
+
+
+class Result(C.Structure):
+    """pdeb200_result (include/pdeb200_server.h)."""
+    _fields_ = [
+        ("id", C.c_int64),
+        ("status", C.c_int32),
+        ("kind", C.c_int32),
+        ("queue_ms", C.c_double),
+        ("run_ms", C.c_double),
+        ("latency_ms", C.c_double),
+        ("iterations", C.c_int32),
+        ("group_size", C.c_int32),
+        ("rel_residual", C.c_double),
+        ("message", C.c_char * 128),
+    ]
+
+
+class ServerStats(C.Structure):
+    """pdeb200_server_stats (include/pdeb200_server.h)."""
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("rejected", C.c_int64),
+        ("in_flight", C.c_int64),
+        ("queued", C.c_int64),
+        ("bytes_in_use", C.c_int64),
+        ("bytes_peak", C.c_int64),
+        ("budget_bytes", C.c_int64),
+        ("lanes_busy_peak", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("p50_ms", C.c_double),
+        ("p99_ms", C.c_double),
+        ("max_ms", C.c_double),
+        ("elapsed_s", C.c_double),
+        ("solves_per_s", C.c_double),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
 FRAME_CB = C.CFUNCTYPE(C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -261,6 +344,18 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_batch_get_options.argtypes = [C.c_void_p, P(BatchOptions)]
     lib.pdeb200_batch_destroy.restype = None
     lib.pdeb200_batch_destroy.argtypes = [C.c_void_p]
+    lib.pdeb200_server_create.restype = C.c_int32
+    lib.pdeb200_server_create.argtypes = [P(ServerOptions), P(C.c_void_p), C.c_char_p, C.c_size_t]
+    lib.pdeb200_server_submit.restype = C.c_int32
+    lib.pdeb200_server_submit.argtypes = [C.c_void_p, P(Request), P(C.c_int64)]
+    lib.pdeb200_server_wait.restype = C.c_int32
+    lib.pdeb200_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double, P(Result)]
+    lib.pdeb200_server_drain.restype = C.c_int32
+    lib.pdeb200_server_drain.argtypes = [C.c_void_p, C.c_double]
+    lib.pdeb200_server_get_stats.restype = C.c_int32
+    lib.pdeb200_server_get_stats.argtypes = [C.c_void_p, P(ServerStats), C.c_int32]
+    lib.pdeb200_server_destroy.restype = None
+    lib.pdeb200_server_destroy.argtypes = [C.c_void_p]
     return lib
 
 

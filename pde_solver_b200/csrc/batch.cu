@@ -97,8 +97,25 @@ long long interior_nodes(const GridDev& g) {
 void make_tiles(const GridDev& g, bool coarse, const BatchParams& p, int lev, int member, std::vector<BTile>* out) {
   const int ni = g.nx - 2, nj = g.ny - 2;
   const int kb = g.dim == 3 ? 1 : 0, ke = g.dim == 3 ? g.nz - 1 : 1;
+  auto tile = [&](int x0, int y0, int w, int h, int z0, int z1, int coarse_flag) {
+    if (w > 65535 || h > 65535) throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "coarsest level too wide for one tile"};
+    BTile t{};
+    t.lev = lev;
+    t.member = member;
+    t.x0 = x0;
+    t.y0 = y0;
+    t.z0 = z0;
+    t.z1 = z1;
+    t.w = (unsigned short)w;
+    t.h = (unsigned short)h;
+    int lw = 0;
+    while ((1 << lw) < w) ++lw;
+    t.lw = (unsigned char)lw;
+    t.coarse = (unsigned char)coarse_flag;
+    out->push_back(t);
+  };
   if (coarse) {
-    out->push_back(BTile{lev, member, 0, 0, ni, nj, kb, ke, 1, 0});
+    tile(0, 0, ni, nj, kb, ke, 1);
     return;
   }
   const int tw = g.dim == 3 ? 32 : p.tile_x;
@@ -106,9 +123,11 @@ void make_tiles(const GridDev& g, bool coarse, const BatchParams& p, int lev, in
   const int tz = g.dim == 3 ? p.tile_z : 1;
   for (int z = kb; z < ke; z += tz)
     for (int y = 0; y < nj; y += th)
-      for (int x = 0; x < ni; x += tw)
-        out->push_back(BTile{lev, member, x, y, std::min(tw, ni - x), std::min(th, nj - y), z, std::min(ke, z + tz),
-                             0, 0});
+      for (int x = 0; x < ni; x += tw) {
+        // regular tiles keep the full row width so a warp stays on one row
+        tile(x, y, std::min(tw, ni - x), std::min(th, nj - y), z, std::min(ke, z + tz), 0);
+        out->back().lw = (unsigned char)(tw == 64 ? 6 : 5);
+      }
 }
 
 template <typename KT>
@@ -575,7 +594,7 @@ void autotune(BatchPlan& B, const pdeb200_batch_options* o) {
     }
   };
   if (has2) {
-    const int shapes[][2] = {{32, 8}, {32, 16}, {32, 32}, {64, 8}, {64, 16}};
+    const int shapes[][2] = {{32, 8}, {32, 16}, {32, 32}, {64, 16}, {64, 32}, {64, 64}};
     const BatchParams base = best;
     for (auto& sh : shapes) {
       if (sh[0] == base.tile_x && sh[1] == base.tile_y) continue;

@@ -12,8 +12,11 @@
 // by the reductions' post steps, so members converge independently and a
 // finished member's tiles return at once.
 //
-// Tiles cover interior nodes only: node (i,j,k) of tile T is
-// i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w, k in [T.z0, T.z1).
+// Tiles cover interior nodes only: tile T holds columns
+// i in [1 + T.x0, 1 + T.x0 + T.w), j in [1 + T.y0, 1 + T.y0 + T.h) and planes
+// k in [T.z0, T.z1). Kernels read the level and member descriptors straight
+// from global memory (one L1 line broadcast to the block), so a block starts
+// streaming its tile without a staging barrier.
 // A member's coarsest level is one whole-grid tile (coarse = 1), solved by
 // the block that restricts into it.
 #pragma once
@@ -72,24 +75,32 @@ struct BMember {
   float* e;
 };
 
-struct BTile {
+struct alignas(16) BTile {
   int lev, member;
-  int x0, y0, w, h;
+  int x0, y0;
   int z0, z1;
-  int coarse;
-  int pad;
+  unsigned short w, h;   // extent in nodes
+  unsigned char lw;      // log2 of the padded row width (w <= 1 << lw)
+  unsigned char coarse;  // whole-grid tile of a coarsest level
+  unsigned char pad[2];
 };
 
-// Copies a descriptor into shared memory (all threads; caller syncs).
-template <class S>
-__device__ __forceinline__ void bstage(S& dst, const S* src) {
-  static_assert(sizeof(S) % 4 == 0, "descriptor size");
-  const int* s = reinterpret_cast<const int*>(src);
-  int* d = reinterpret_cast<int*>(&dst);
-  for (int t = threadIdx.x; t < (int)(sizeof(S) / 4); t += blockDim.x) d[t] = __ldg(s + t);
+// Visits the (i,j) columns of tile T that this thread owns: thread t takes
+// column t & (W-1) of row t >> lw (W = 1 << lw), so a warp covers 32
+// consecutive nodes of a row.
+template <class F>
+__device__ __forceinline__ void tile_columns(const BTile& T, F&& f) {
+  const int mask = (1 << T.lw) - 1;
+  const int total = int(T.h) << T.lw;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int a = t & mask;
+    if (a >= int(T.w)) continue;
+    f(1 + T.x0 + a, 1 + T.y0 + (t >> T.lw));
+  }
 }
 
-__device__ __forceinline__ int bstate(const BMember* m) { return *((volatile const int*)&m->state); }
+// Member fields written by the post steps are read with L2-coherent loads.
+__device__ __forceinline__ int bstate(const BMember* m) { return __ldcg(&m->state); }
 __device__ __forceinline__ bool vcycle_state(int s) { return s == kBInnerStart || s == kBInnerRun; }
 
 // Folded stencil of interior node (i,j,kk) of level L with coefficient field k.
@@ -232,40 +243,38 @@ constexpr int kBThreads = 256;
 __global__ void __launch_bounds__(kBThreads) kb_rhs(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
                                                     const BMember* __restrict__ mem) {
   const BTile T = tiles[blockIdx.x];
-  __shared__ BLevel L;
-  bstage(L, lv + T.lev);
-  __syncthreads();
+  const BLevel& L = lv[T.lev];
   const BMember& m = mem[T.member];
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const double* k64 = m.k64;
+  const double* f64 = m.f64;
+  double* b64 = m.b64;
+  double* x64 = m.x64;
+  tile_columns(T, [&](int i, int j) {
     for (int kk = T.z0; kk < T.z1; ++kk) {
       const long long id = bid(L.g, i, j, kk);
       double sh = 0.0;
-      (void)bstencil<double, double>(L, m.k64, i, j, kk, id, &sh);
-      m.b64[id] = -(m.f64 ? m.f64[id] : 0.0) - sh;
-      m.x64[id] = 0.0;
+      (void)bstencil<double, double>(L, k64, i, j, kk, id, &sh);
+      b64[id] = -(f64 ? f64[id] : 0.0) - sh;
+      x64[id] = 0.0;
     }
-  }
+  });
 }
 
 // x64 += e for members about to take an outer step with a pending correction.
 __global__ void __launch_bounds__(kBThreads) kb_xupdate(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
-                                                        const BMember* __restrict__ mem) {
+                                                        const BMember* mem) {
   const BTile T = tiles[blockIdx.x];
   const BMember* m = mem + T.member;
-  if (bstate(m) != kBNeedOuter || !*((volatile const int*)&m->e_valid)) return;
+  if (bstate(m) != kBNeedOuter || !__ldcg(&m->e_valid)) return;
   const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
-  double* x = m->x64;
-  const float* e = m->e;
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  double* __restrict__ x = m->x64;
+  const float* __restrict__ e = m->e;
+  tile_columns(T, [&](int i, int j) {
     for (int kk = T.z0; kk < T.z1; ++kk) {
       const long long id = ((long long)kk * ny + j) * nx + i;
       x[id] += double(e[id]);
     }
-  }
+  });
 }
 
 // Outer FP64 residual r = b - A x; the FP32 copy is the inner right-hand side.
@@ -274,20 +283,16 @@ __global__ void __launch_bounds__(kBThreads) kb_outer(const BTile* __restrict__ 
   const BTile T = tiles[blockIdx.x];
   BMember* m = mem + T.member;
   if (bstate(m) != kBNeedOuter) return;
-  __shared__ BLevel L;
-  bstage(L, lv + T.lev);
-  __syncthreads();
+  const BLevel& L = lv[T.lev];
   const double* __restrict__ x = m->x64;
   const double* __restrict__ b = m->b64;
   float* __restrict__ r32 = L.b;
   const double* k64 = m->k64;
-  double acc[1] = {0.0};
-  const int cols = T.w * T.h;
-  const int nx = L.g.nx;
+  const int nx = L.g.nx, dim = L.g.dim;
   const long long sxy = L.g.sxy;
-  const bool is3 = L.g.dim == 3;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const bool is3 = dim == 3;
+  double acc[1] = {0.0};
+  tile_columns(T, [&](int i, int j) {
     long long id = bid(L.g, i, j, T.z0);
     double zm = is3 ? x[id - sxy] : 0.0;
     double zc = x[id];
@@ -295,13 +300,13 @@ __global__ void __launch_bounds__(kBThreads) kb_outer(const BTile* __restrict__ 
       const double zp = is3 ? x[id + sxy] : 0.0;
       const Stencil<double> s = bstencil<double, double>(L, k64, i, j, kk, id, nullptr);
       const double v = b[id] - (s.c * zc + nb_sum<double>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm,
-                                                           L.g.dim));
+                                                           dim));
       r32[id] = float(v);
       acc[0] += v * v;
       zm = zc;
       zc = zp;
     }
-  }
+  });
   member_reduce<1>(acc, partials, m, blockIdx.x, BPostOuter{active});
 }
 
@@ -312,32 +317,28 @@ __global__ void __launch_bounds__(kBThreads) kb_apply_pq(const BTile* __restrict
   const BTile T = tiles[blockIdx.x];
   BMember* m = mem + T.member;
   if (bstate(m) != kBInnerRun) return;
-  __shared__ BLevel L;
-  bstage(L, lv + T.lev);
-  __syncthreads();
+  const BLevel& L = lv[T.lev];
   const float* __restrict__ p = m->p;
   float* __restrict__ q = m->q;
   const float* k32 = m->k32;
-  double acc[1] = {0.0};
-  const int cols = T.w * T.h;
-  const int nx = L.g.nx;
+  const int nx = L.g.nx, dim = L.g.dim;
   const long long sxy = L.g.sxy;
-  const bool is3 = L.g.dim == 3;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const bool is3 = dim == 3;
+  double acc[1] = {0.0};
+  tile_columns(T, [&](int i, int j) {
     long long id = bid(L.g, i, j, T.z0);
     float zm = is3 ? p[id - sxy] : 0.f;
     float zc = p[id];
     for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
       const float zp = is3 ? p[id + sxy] : 0.f;
       const Stencil<float> s = bstencil<float, float>(L, k32, i, j, kk, id, nullptr);
-      const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, L.g.dim);
+      const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, dim);
       q[id] = v;
       acc[0] += double(zc) * double(v);
       zm = zc;
       zc = zp;
     }
-  }
+  });
   member_reduce<1>(acc, partials, m, blockIdx.x, BPostPQ{});
 }
 
@@ -352,12 +353,10 @@ __global__ void __launch_bounds__(kBThreads) kb_update(const BTile* __restrict__
   const float* __restrict__ p = m->p;
   const float* __restrict__ q = m->q;
   float* __restrict__ e = m->e;
-  const float a = float(*((volatile const double*)&m->alpha));
-  const bool first = *((volatile const int*)&m->inner) == 0;
+  const float a = float(__ldcg(&m->alpha));
+  const bool first = __ldcg(&m->inner) == 0;
   double acc[1] = {0.0};
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  tile_columns(T, [&](int i, int j) {
     for (int kk = T.z0; kk < T.z1; ++kk) {
       const long long id = ((long long)kk * ny + j) * nx + i;
       e[id] = first ? a * p[id] : e[id] + a * p[id];
@@ -365,7 +364,7 @@ __global__ void __launch_bounds__(kBThreads) kb_update(const BTile* __restrict__
       r[id] = rv;
       acc[0] += double(rv) * double(rv);
     }
-  }
+  });
   member_reduce<1>(acc, partials, m, blockIdx.x, BPostUpdate{});
 }
 
@@ -379,14 +378,12 @@ __global__ void __launch_bounds__(kBThreads) kb_rz(const BTile* __restrict__ til
   const float* __restrict__ r = lv[T.lev].b;
   const float* __restrict__ z = lv[T.lev].x;
   double acc[1] = {0.0};
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  tile_columns(T, [&](int i, int j) {
     for (int kk = T.z0; kk < T.z1; ++kk) {
       const long long id = ((long long)kk * ny + j) * nx + i;
       acc[0] += double(r[id]) * double(z[id]);
     }
-  }
+  });
   member_reduce<1>(acc, partials, m, blockIdx.x, BPostRZ{});
 }
 
@@ -399,16 +396,14 @@ __global__ void __launch_bounds__(kBThreads) kb_pupdate(const BTile* __restrict_
   const int nx = lv[T.lev].g.nx, ny = lv[T.lev].g.ny;
   const float* __restrict__ z = lv[T.lev].x;
   float* __restrict__ p = m->p;
-  const bool first = *((volatile const int*)&m->first) != 0;
-  const float bt = float(*((volatile const double*)&m->beta));
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const bool first = __ldcg(&m->first) != 0;
+  const float bt = float(__ldcg(&m->beta));
+  tile_columns(T, [&](int i, int j) {
     for (int kk = T.z0; kk < T.z1; ++kk) {
       const long long id = ((long long)kk * ny + j) * nx + i;
       p[id] = first ? z[id] : z[id] + bt * p[id];
     }
-  }
+  });
 }
 
 // One red-black colour pass of the V-cycle smoother on level tiles. from_zero:
@@ -420,18 +415,14 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
   if (!vcycle_state(bstate(mem + T.member))) return;
-  __shared__ BLevel L;
-  bstage(L, lv + T.lev);
-  __syncthreads();
+  const BLevel& L = lv[T.lev];
   const KT* k = static_cast<const KT*>(L.kh);
   float* __restrict__ x = L.x;
   const float* __restrict__ b = L.b;
-  const int nx = L.g.nx;
+  const int nx = L.g.nx, dim = L.g.dim;
   const long long sxy = L.g.sxy;
-  const bool is3 = L.g.dim == 3;
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const bool is3 = dim == 3;
+  tile_columns(T, [&](int i, int j) {
     if (from_zero) {
       for (int kk = T.z0; kk < T.z1; ++kk) {
         const long long id = bid(L.g, i, j, kk);
@@ -448,10 +439,10 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
         const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
         const float zp = is3 ? x[id + sxy] : 0.f;
         const float zm = is3 ? x[id - sxy] : 0.f;
-        x[id] = (b[id] - nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, L.g.dim)) / s.c;
+        x[id] = (b[id] - nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, dim)) / s.c;
       }
     }
-  }
+  });
 }
 
 // Level residual r = b - A x on level tiles.
@@ -461,30 +452,26 @@ __global__ void __launch_bounds__(kBThreads) kb_residual(const BTile* __restrict
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
   if (!vcycle_state(bstate(mem + T.member))) return;
-  __shared__ BLevel L;
-  bstage(L, lv + T.lev);
-  __syncthreads();
+  const BLevel& L = lv[T.lev];
   const KT* k = static_cast<const KT*>(L.kh);
   const float* __restrict__ x = L.x;
   const float* __restrict__ b = L.b;
   float* __restrict__ r = L.r;
-  const int nx = L.g.nx;
+  const int nx = L.g.nx, dim = L.g.dim;
   const long long sxy = L.g.sxy;
-  const bool is3 = L.g.dim == 3;
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  const bool is3 = dim == 3;
+  tile_columns(T, [&](int i, int j) {
     long long id = bid(L.g, i, j, T.z0);
     float zm = is3 ? x[id - sxy] : 0.f;
     float zc = x[id];
     for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
       const float zp = is3 ? x[id + sxy] : 0.f;
       const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
-      r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, L.g.dim));
+      r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, dim));
       zm = zc;
       zc = zp;
     }
-  }
+  });
 }
 
 // Coarsest-level solve inside one block: `sweeps` red-black sweeps from zero
@@ -501,12 +488,14 @@ __device__ void bcoarse_solve(const BLevel& C, int sweeps) {
   const int ni = g.nx - 2, nj = g.ny - 2, nk = ke - kb;
   const int total = ni * nj * nk;
   const bool smem = g.n <= kBCoarseSmem;
+  float* x = C.x;
+  const float* b = C.b;
   if (smem) {
     for (int t = threadIdx.x; t < (int)g.n; t += blockDim.x) cs[t] = 0.0;
   } else {
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
       const int i = 1 + t % ni, j = 1 + (t / ni) % nj, kk = kb + t / (ni * nj);
-      C.x[bid(g, i, j, kk)] = 0.f;
+      x[bid(g, i, j, kk)] = 0.f;
     }
   }
   __syncthreads();
@@ -522,13 +511,12 @@ __device__ void bcoarse_solve(const BLevel& C, int sweeps) {
           const int q = (int)id, nx = g.nx, sxy = (int)g.sxy;
           v = st.xp * cs[q + 1] + st.xm * cs[q - 1] + st.yp * cs[q + nx] + st.ym * cs[q - nx];
           if (g.dim == 3) v += st.zp * cs[q + sxy] + st.zm * cs[q - sxy];
-          cs[q] = (double(C.b[id]) - v) / st.c;
+          cs[q] = (double(b[id]) - v) / st.c;
         } else {
-          const float* x = C.x;
           v = st.xp * double(x[id + 1]) + st.xm * double(x[id - 1]) + st.yp * double(x[id + g.nx]) +
               st.ym * double(x[id - g.nx]);
           if (g.dim == 3) v += st.zp * double(x[id + g.sxy]) + st.zm * double(x[id - g.sxy]);
-          C.x[id] = float((double(C.b[id]) - v) / st.c);
+          x[id] = float((double(b[id]) - v) / st.c);
         }
       }
       __syncthreads();
@@ -537,7 +525,7 @@ __device__ void bcoarse_solve(const BLevel& C, int sweeps) {
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
       const int i = 1 + t % ni, j = 1 + (t / ni) % nj, kk = kb + t / (ni * nj);
       const long long id = bid(g, i, j, kk);
-      C.x[id] = float(cs[id]);
+      x[id] = float(cs[id]);
     }
 }
 
@@ -551,20 +539,16 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
                                                          int coarse_sweeps) {
   const BTile T = tiles[blockIdx.x];
   if (!vcycle_state(bstate(mem + T.member))) return;
-  __shared__ BLevel C;
-  __shared__ BLevel F;
-  bstage(C, lv + T.lev);
-  __syncthreads();
-  bstage(F, lv + C.prev);
-  __syncthreads();
+  const BLevel& C = lv[T.lev];
+  const BLevel& F = lv[C.prev];
   const GridDev& gc = C.g;
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int I = 1 + T.x0 + t % T.w, J = 1 + T.y0 + t / T.w;
+  const float* __restrict__ rf = F.r;
+  float* __restrict__ bc = C.b;
+  tile_columns(T, [&](int I, int J) {
     const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
     const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
     for (int K = T.z0; K < T.z1; ++K) {
-      double acc = full_weight<float>(F.g, gc, F.r, I, J, K);
+      double acc = full_weight<float>(F.g, gc, rf, I, J, K);
       const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
       if (dxl | dxh | dyl | dyh | dzl | dzh) {
         for (int dk = dzl; dk <= dzh; ++dk)
@@ -574,12 +558,12 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
               int ci = I + di, cj = J + dj, ck = K + dk;
               const double coef = ext_chain(gc, ci, cj, ck);
               if (coef != 0.0 && ci == I && cj == J && ck == K)
-                acc += coef * full_weight<float>(F.g, gc, F.r, I + di, J + dj, K + dk);
+                acc += coef * full_weight<float>(F.g, gc, rf, I + di, J + dj, K + dk);
             }
       }
-      C.b[bid(gc, I, J, K)] = float(acc);
+      bc[bid(gc, I, J, K)] = float(acc);
     }
-  }
+  });
   if (T.coarse) {
     __syncthreads();
     bcoarse_solve<KT>(C, coarse_sweeps);
@@ -592,21 +576,15 @@ __global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict_
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
   if (!vcycle_state(bstate(mem + T.member))) return;
-  __shared__ BLevel F;
-  __shared__ BLevel C;
-  bstage(F, lv + T.lev);
-  __syncthreads();
-  bstage(C, lv + F.next);
-  __syncthreads();
+  const BLevel& F = lv[T.lev];
+  const BLevel& C = lv[F.next];
   const GridDev& gf = F.g;
   const GridDev& gc = C.g;
   const float* __restrict__ xc = C.x;
   float* __restrict__ xf = F.x;
   const int xmode = map_mode(gf.nx, gc.nx), ymode = map_mode(gf.ny, gc.ny);
   const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
-  const int cols = T.w * T.h;
-  for (int t = threadIdx.x; t < cols; t += blockDim.x) {
-    const int i = 1 + T.x0 + t % T.w, j = 1 + T.y0 + t / T.w;
+  tile_columns(T, [&](int i, int j) {
     int I0, J0;
     double tx, ty;
     coarse_pos(i, gf.nx, gc.nx, xmode, I0, tx);
@@ -649,7 +627,7 @@ __global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict_
       const long long id = bid(gf, i, j, k);
       xf[id] = float(double(xf[id]) + v);
     }
-  }
+  });
 }
 
 // Boundary nodes of each member's FP64 solution from the closures (reference
@@ -657,10 +635,7 @@ __global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict_
 __global__ void __launch_bounds__(kBThreads) kb_fill_boundary(const BLevel* __restrict__ lv,
                                                               const BMember* __restrict__ mem) {
   const BMember* m = mem + blockIdx.x;
-  __shared__ BLevel L;
-  bstage(L, lv + m->level0);
-  __syncthreads();
-  const GridDev& g = L.g;
+  const GridDev& g = lv[m->level0].g;
   double* u = m->x64;
   const long long nyz = (long long)g.ny * g.nz, nxz = (long long)g.nx * g.nz, nxy = (long long)g.nx * g.ny;
   const long long total = 2 * nyz + 2 * nxz + (g.dim == 3 ? 2 * nxy : 0);

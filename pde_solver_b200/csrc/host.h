@@ -179,6 +179,10 @@ inline double interior_dofs(const GridDev& g) {
 }
 
 Context* get_context(int dev);  // throws StatusFailure / CudaFailure
+// A context of one's own (stream, control block, reduction buffers): callers
+// that run solves concurrently on one device give each thread its own.
+void init_context(Context* c, int dev);
+void free_context(Context* c);
 void release_contexts();
 
 // Device copy of a problem, with face closures materialised.
@@ -238,6 +242,11 @@ void set_report_msg(pdeb200_report* r, const std::string& m);
 // Solver drivers (solvers.cu)
 pdeb200_status solve_dispatch(Context* ctx, DevProblem& P, const pdeb200_problem* hp, const pdeb200_options* o,
                               double* d_out, pdeb200_report* rep);
+// Host-array entry bodies on a given context (the caller serialises use of ctx).
+pdeb200_status solve_on(Context* ctx, const pdeb200_problem* prob, const pdeb200_options* opt, double* out_grid,
+                        pdeb200_report* report);
+pdeb200_status time_series_on(Context* ctx, const pdeb200_problem* prob, const pdeb200_time_options* topt,
+                              pdeb200_frame_cb on_frame, void* user, double* out_grid, pdeb200_report* report);
 pdeb200_status residual_norms_dev(Context* ctx, DevProblem& P, const double* d_grid, double* l2, double* linf);
 pdeb200_status apply_dev(Context* ctx, DevProblem& P, const double* d_x, double* d_y);
 pdeb200_status time_series_dev(Context* ctx, DevProblem& P, const pdeb200_time_options* t, pdeb200_frame_cb cb,

@@ -29,48 +29,64 @@ Context* get_context(int dev) {
   PDEB_CUDA(cudaSetDevice(dev));
   if (!g_ctx[dev]) {
     auto c = std::make_unique<Context>();
-    c->dev = dev;
-    cudaDeviceProp prop;
-    PDEB_CUDA(cudaGetDeviceProperties(&prop, dev));
-    c->name = prop.name;
-    c->num_sms = prop.multiProcessorCount;
-    PDEB_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
-    c->stream = c->own_stream;
-    PDEB_CUDA(cudaEventCreate(&c->ev0));
-    PDEB_CUDA(cudaEventCreate(&c->ev1));
-    PDEB_CUDA(cudaMalloc(&c->d_ctl, sizeof(Ctl)));
-    PDEB_CUDA(cudaMallocHost(&c->h_ctl, sizeof(Ctl)));
-    c->max_blocks = kMaxGridBlocks;
-    const int nslots = 4;
-    PDEB_CUDA(cudaMalloc(&c->d_partials, sizeof(double) * c->max_blocks * kMaxRed * nslots));
-    PDEB_CUDA(cudaMalloc(&c->d_tickets, sizeof(unsigned) * nslots));
-    PDEB_CUDA(cudaMemset(c->d_tickets, 0, sizeof(unsigned) * nslots));
-    PDEB_CUDA(cudaMalloc(&c->d_redout, sizeof(double) * kMaxRed * nslots));
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t thr = std::numeric_limits<uint64_t>::max();
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
+    init_context(c.get(), dev);
     g_ctx[dev] = std::move(c);
   }
   return g_ctx[dev].get();
+}
+
+void init_context(Context* c, int dev) {
+  PDEB_CUDA(cudaSetDevice(dev));
+  c->dev = dev;
+  cudaDeviceProp prop;
+  PDEB_CUDA(cudaGetDeviceProperties(&prop, dev));
+  c->name = prop.name;
+  c->num_sms = prop.multiProcessorCount;
+  PDEB_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+  c->stream = c->own_stream;
+  PDEB_CUDA(cudaEventCreate(&c->ev0));
+  PDEB_CUDA(cudaEventCreate(&c->ev1));
+  PDEB_CUDA(cudaMalloc(&c->d_ctl, sizeof(Ctl)));
+  PDEB_CUDA(cudaMallocHost(&c->h_ctl, sizeof(Ctl)));
+  c->max_blocks = kMaxGridBlocks;
+  const int nslots = 4;
+  PDEB_CUDA(cudaMalloc(&c->d_partials, sizeof(double) * c->max_blocks * kMaxRed * nslots));
+  PDEB_CUDA(cudaMalloc(&c->d_tickets, sizeof(unsigned) * nslots));
+  PDEB_CUDA(cudaMemset(c->d_tickets, 0, sizeof(unsigned) * nslots));
+  PDEB_CUDA(cudaMalloc(&c->d_redout, sizeof(double) * kMaxRed * nslots));
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = std::numeric_limits<uint64_t>::max();
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+}
+
+void free_context(Context* c) {
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_ctl);
+  cudaFreeHost(c->h_ctl);
+  cudaFree(c->d_partials);
+  cudaFree(c->d_tickets);
+  cudaFree(c->d_redout);
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  for (auto e : c->evpool) cudaEventDestroy(e);
+  c->evpool.clear();
+  cudaStreamDestroy(c->own_stream);
+  c->d_ctl = nullptr;
+  c->h_ctl = nullptr;
+  c->d_partials = nullptr;
+  c->d_tickets = nullptr;
+  c->d_redout = nullptr;
+  c->own_stream = c->stream = nullptr;
 }
 
 void release_contexts() {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   for (auto& c : g_ctx) {
     if (!c) continue;
-    cudaSetDevice(c->dev);
-    cudaStreamSynchronize(c->stream);
-    cudaFree(c->d_ctl);
-    cudaFreeHost(c->h_ctl);
-    cudaFree(c->d_partials);
-    cudaFree(c->d_tickets);
-    cudaFree(c->d_redout);
-    cudaEventDestroy(c->ev0);
-    cudaEventDestroy(c->ev1);
-    for (auto e : c->evpool) cudaEventDestroy(e);
-    cudaStreamDestroy(c->own_stream);
+    free_context(c.get());
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, c->dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     c.reset();
@@ -334,6 +350,48 @@ void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
   }
 }
 
+pdeb200_status solve_on(Context* ctx, const pdeb200_problem* prob, const pdeb200_options* opt, double* out_grid,
+                        pdeb200_report* report) {
+  ctx->launches = 0;
+  DevProblem P;
+  upload_problem(ctx, prob, &P);
+  const long long n = P.g.n;
+  double* d_out = out_grid;
+  Buf out_buf;
+  if (!P.device_inputs) {
+    out_buf = Buf(sizeof(double) * n, ctx->stream);
+    d_out = out_buf.as<double>();
+  }
+  pdeb200_status s = solve_dispatch(ctx, P, prob, opt, d_out, report);
+  if (!P.device_inputs && (s == PDEB200_OK || s == PDEB200_ERR_NOT_CONVERGED))
+    PDEB_CUDA(cudaMemcpyAsync(out_grid, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  PDEB_CUDA(cudaGetLastError());
+  ctx->prof_flush();
+  if (report) report->kernel_launches = (int32_t)ctx->launches;
+  return s;
+}
+
+pdeb200_status time_series_on(Context* ctx, const pdeb200_problem* prob, const pdeb200_time_options* topt,
+                              pdeb200_frame_cb on_frame, void* user, double* out_grid, pdeb200_report* report) {
+  ctx->launches = 0;
+  DevProblem P;
+  upload_problem(ctx, prob, &P);
+  const long long n = P.g.n;
+  double* d_out = out_grid;
+  Buf ob;
+  if (!P.device_inputs) {
+    ob = Buf(sizeof(double) * n, ctx->stream);
+    d_out = ob.as<double>();
+  }
+  pdeb200_status s = time_series_dev(ctx, P, topt, on_frame, user, !P.device_inputs, d_out, report);
+  if (!P.device_inputs && s == PDEB200_OK)
+    PDEB_CUDA(cudaMemcpyAsync(out_grid, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (report) report->kernel_launches = (int32_t)ctx->launches;
+  return s;
+}
+
 void set_report_msg(pdeb200_report* r, const std::string& m) {
   if (!r) return;
   std::strncpy(r->message, m.c_str(), sizeof(r->message) - 1);
@@ -486,24 +544,7 @@ pdeb200_status pdeb200_solve(const pdeb200_problem* prob, const pdeb200_options*
   pdeb200_status st = guarded(report, [&]() -> pdeb200_status {
     Context* ctx = get_context(opt->device);
     std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->launches = 0;
-    DevProblem P;
-    upload_problem(ctx, prob, &P);
-    const long long n = P.g.n;
-    double* d_out = out_grid;
-    Buf out_buf;
-    if (!P.device_inputs) {
-      out_buf = Buf(sizeof(double) * n, ctx->stream);
-      d_out = out_buf.as<double>();
-    }
-    pdeb200_status s = solve_dispatch(ctx, P, prob, opt, d_out, report);
-    if (!P.device_inputs && (s == PDEB200_OK || s == PDEB200_ERR_NOT_CONVERGED))
-      PDEB_CUDA(cudaMemcpyAsync(out_grid, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
-    PDEB_CUDA(cudaGetLastError());
-    ctx->prof_flush();
-    if (report) report->kernel_launches = (int32_t)ctx->launches;
-    return s;
+    return solve_on(ctx, prob, opt, out_grid, report);
   });
   if (report) {
     report->total_ms = now_ms() - t0;
@@ -568,22 +609,7 @@ pdeb200_status pdeb200_time_series(const pdeb200_problem* prob, const pdeb200_ti
   pdeb200_status st = guarded(report, [&]() -> pdeb200_status {
     Context* ctx = get_context(topt->device);
     std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->launches = 0;
-    DevProblem P;
-    upload_problem(ctx, prob, &P);
-    const long long n = P.g.n;
-    double* d_out = out_grid;
-    Buf ob;
-    if (!P.device_inputs) {
-      ob = Buf(sizeof(double) * n, ctx->stream);
-      d_out = ob.as<double>();
-    }
-    pdeb200_status s = time_series_dev(ctx, P, topt, on_frame, user, !P.device_inputs, d_out, report);
-    if (!P.device_inputs && s == PDEB200_OK)
-      PDEB_CUDA(cudaMemcpyAsync(out_grid, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (report) report->kernel_launches = (int32_t)ctx->launches;
-    return s;
+    return time_series_on(ctx, prob, topt, on_frame, user, out_grid, report);
   });
   if (report) report->total_ms = now_ms() - t0;
   return st;

@@ -105,3 +105,64 @@ def batch_members(n2d: int = 2048, n3d: int = 256, seed: int = 4242, sigma: floa
         p.f = (-rng.standard_normal(shape)).reshape(-1)
         out.append(p)
     return out
+
+
+def gaussian_bump(p: GridProblem, width: float = 40.0) -> np.ndarray:
+    """u0 = exp(-width |x - c|^2) around the domain centre."""
+    x, y, z = p.coords()
+    x0, x1, y0, y1, z0, z1 = p.bounds
+    r2 = (x - 0.5 * (x0 + x1)) ** 2 + (y - 0.5 * (y0 + y1)) ** 2
+    if p.nz > 1:
+        r2 = r2 + (z - 0.5 * (z0 + z1)) ** 2
+    return np.ascontiguousarray(np.broadcast_to(np.exp(-width * r2), (max(p.nz, 1), p.ny, p.nx))).reshape(-1)
+
+
+def heat_problem(n: int, dim: int = 2) -> tuple:
+    """u_t = Laplace(u) (reference form a=b[=az]=-1, ut=1), Dirichlet 0, Gaussian
+    bump u0; returns (problem, dt) with dt = 0.9 h^2 / (2 dim), the forward-Euler
+    limit scaled by 0.9."""
+    p = GridProblem(n, n, n if dim == 3 else 1, a=-1.0, b=-1.0, az=-1.0 if dim == 3 else 0.0, ut=1.0)
+    p.u0 = gaussian_bump(p)
+    h = 1.0 / (n - 1)
+    return p, 0.9 * h * h / (2 * dim)
+
+
+def projection_fields(n: int, seed: int) -> tuple:
+    """2D velocity (u, v) ~ N(0,1) and zero pressure on an n x n grid."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return rng.standard_normal(n * n), rng.standard_normal(n * n), np.zeros(n * n)
+
+
+def serving_requests(count: int, seed: int, rate_hz: float, lo2=65, hi2=513, lo3=65, hi3=129,
+                     heat_hi=257, proj_lo=256, proj_hi=1024, mix=(0.6, 0.25, 0.15)) -> list:
+    """A seeded request stream: (arrival_s, kind, spec) with Poisson-process
+    arrivals at `rate_hz`; kinds drawn with probabilities `mix` (Poisson solve,
+    200-step heat, 2D projection). Poisson solves are 2D (sides lo2..hi2) or 3D
+    (sides lo3..hi3) divergence-form problems with k log-normal sigma=0.5."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for q in range(count):
+        t += rng.exponential(1.0 / rate_hz)
+        kind = rng.choice(3, p=mix)
+        if kind == 0:
+            is3 = rng.random() < 0.3
+            lo, hi = (lo3, hi3) if is3 else (lo2, hi2)
+            n = int(np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+            out.append((t, "poisson", dict(n=n, dim=3 if is3 else 2, seed=int(rng.integers(1 << 30)))))
+        elif kind == 1:
+            n = int(np.rint(np.exp(rng.uniform(np.log(lo2), np.log(heat_hi)))))
+            out.append((t, "heat", dict(n=n, steps=200)))
+        else:
+            n = int(np.rint(np.exp(rng.uniform(np.log(proj_lo), np.log(proj_hi)))))
+            out.append((t, "projection", dict(n=n, seed=int(rng.integers(1 << 30)))))
+    return out
+
+
+def poisson_request_problem(n: int, dim: int, seed: int, sigma: float = 0.5) -> GridProblem:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shape = (n, n, n) if dim == 3 else (n, n)
+    p = GridProblem(n, n, n if dim == 3 else 1, coef_kind=abi.COEF_DIVK)
+    p.k = np.exp(sigma * rng.standard_normal(shape)).reshape(-1)
+    p.f = (-rng.standard_normal(shape)).reshape(-1)
+    return p

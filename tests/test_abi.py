@@ -31,7 +31,8 @@ def test_abi_version(lib):
 
 @pytest.mark.parametrize("which,cls", [(0, abi.Face), (1, abi.Problem), (2, abi.Options), (3, abi.Report),
                                        (4, abi.TimeOptions), (5, abi.ProjectionOptions), (6, abi.ProjectionReport),
-                                       (7, abi.BatchOptions), (8, abi.BatchStats)])
+                                       (7, abi.BatchOptions), (8, abi.BatchStats), (9, abi.ServerOptions),
+                                       (10, abi.Request), (11, abi.Result), (12, abi.ServerStats)])
 def test_struct_layout_matches_header(oracle_mod, which, cls):
     assert oracle_mod.restate().rs_sizeof(which) == C.sizeof(cls)
 
