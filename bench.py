@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and serving measurements")
     return ap.parse_args()
 
 
@@ -154,6 +155,97 @@ def cpu_sample(prob, gpu_iters):
             "sample": (f"oracle/restate.c MG-PCG on the same {prob.nx}^3 input, OpenMP {cores} threads: "
                        f"setup+1 and setup+3 iterations timed ({times[1]:.2f}s, {times[3]:.2f}s), "
                        f"solve = setup + {gpu_iters} iterations = {t_solve:.2f}s")}
+
+
+TUNE_CACHE = os.path.join(ROOT, "pde_solver_b200", "batch_tune_cache.txt")
+
+
+def bench_batched(lib, abi, n2d=2048, n3d=256, reps=3):
+    """Batched form: 2048 2D grids (sides log-uniform in [33, 513]) and 256 3D
+    grids (sides log-uniform in [17, 129]), k log-normal sigma=0.5, f ~ N(0,1),
+    Dirichlet 0; FP32 MG-PCG in FP64 refinement to 1e-10 for every member; the
+    schedule comes from the autotuner's cache. Compared with the plain FP64
+    MG-PCG path (one pdeb200_solve per grid) on an evenly spaced sample."""
+    import torch
+
+    from pde_solver_b200 import synthetic
+    from pde_solver_b200.batch import Batch
+    from pde_solver_b200.problem import default_options
+
+    ms = synthetic.batch_members(n2d, n3d)
+    t0 = time.perf_counter()
+    b = Batch(ms, autotune=1, tune_cache=TUNE_CACHE)
+    create_s = time.perf_counter() - t0
+    b.solve(1e-10)
+    dev = []
+    for _ in range(reps):
+        reps_ = b.solve(1e-10)
+        dev.append(b.stats.device_ms)
+    st = b.stats
+    worst = max(r.rel_residual for r in reps_)
+    o = b.options()
+    # end to end: packed f from pinned host memory in, packed solution out
+    nodes = b.nodes
+    f_host = torch.from_numpy(np.concatenate([p.f for p in ms])).pin_memory()
+    x_host = torch.empty(nodes, dtype=torch.float64).pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        lib.pdeb200_batch_load_rhs(b.handle, C.c_void_p(f_host.data_ptr()), abi.MEM_HOST)
+        b.solve(1e-10)
+        lib.pdeb200_batch_read(b.handle, C.c_void_p(x_host.data_ptr()), abi.MEM_HOST)
+    e2e_s = (time.perf_counter() - t0) / reps
+    b.close()
+    # plain FP64 path on every 36th member
+    opt = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400)
+    from pde_solver_b200 import solver
+
+    sample = ms[::36]
+    solver.solve(sample[0], opt)
+    plain_ms = 0.0
+    for p in sample:
+        _, r = solver.solve(p, opt)
+        plain_ms += r.device_ms
+    plain_rate = len(sample) / (plain_ms / 1e3)
+    batched_rate = len(ms) / (statistics.median(dev) / 1e3)
+    return {"workload": f"{n2d} 2D grids (sides 33..513) + {n3d} 3D grids (sides 17..129), var-k Poisson",
+            "members": len(ms), "nodes": nodes, "precision": "FP32 MG-PCG in FP64 refinement, tol 1e-10",
+            "solves_per_s": batched_rate, "ms_per_batch": statistics.median(dev),
+            "e2e_solves_per_s": len(ms) / e2e_s, "e2e_h2d_bytes": nodes * 8, "e2e_d2h_bytes": nodes * 8,
+            "worst_rel_residual": worst, "converged": st.converged, "cycles": st.cycles,
+            "kernel_launches": st.kernel_launches, "device_gb": st.device_bytes / 1e9, "create_s": create_s,
+            "schedule": {"tile": [o.tile_x, o.tile_y, o.tile_z], "pre": o.pre_smooth, "post": o.post_smooth,
+                         "inner_tol": o.inner_tol, "from_cache": bool(st.tuned_from_cache)},
+            "plain_fp64_solves_per_s": plain_rate, "plain_fp64_sample": len(sample),
+            "speedup_vs_plain_fp64": batched_rate / plain_rate}
+
+
+def bench_serving(abi, count=256, seed=7):
+    """Serving form: a stream of Poisson requests (2D sides 65..513, 3D sides
+    65..129, k log-normal sigma=0.5) submitted at once (saturation) to a
+    4-lane server, mixed precision (continuous batching) vs the plain FP64
+    path; latency is submit -> result written to host memory."""
+    from pde_solver_b200 import synthetic
+    from pde_solver_b200.server import Server
+
+    reqs = [s for s in synthetic.serving_requests(count, seed=seed, rate_hz=1e9, mix=(1.0, 0.0, 0.0))]
+    probs = [synthetic.poisson_request_problem(sp["n"], sp["dim"], sp["seed"]) for _, _, sp in reqs]
+    out = {}
+    for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
+        with Server(lanes=4, precision=prec, tile_x=64, tile_y=64, tile_z=32, pre_smooth=1, post_smooth=2,
+                    inner_tol=1e-5) as s:
+            s.wait(s.submit_poisson(probs[0]))
+            s.stats(reset=True)
+            t0 = time.perf_counter()
+            ids = [s.submit_poisson(p) for p in probs]
+            res = [s.wait(i)[1] for i in ids]
+            wall = time.perf_counter() - t0
+            st = s.stats()
+        out[name] = {"solves_per_s": len(probs) / wall, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                     "failed": int(sum(r.status != abi.OK for r in res)),
+                     "max_group": int(max(r.group_size for r in res))}
+    out["workload"] = f"{count} Poisson requests at saturation (2D 65..513, 3D 65..129), tol 1e-10"
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    return out
 
 
 def run_reference(args):
@@ -362,6 +454,11 @@ def main():
                 "matches_device_result": bool(ok_host)},
         "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
     }
+    if rank == 0 and world == 1 and not args.no_forms:
+        try:
+            line["forms"] = {"batched": bench_batched(lib, abi), "serving": bench_serving(abi)}
+        except Exception as exc:  # the forms never block the headline line
+            line["forms"] = {"error": str(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_sample(prob, iters)

@@ -300,23 +300,51 @@ int solve_all(BatchPlan& B, double tol, int max_cycles_cap = 0) {
 
 // ------------------------------------------------------------ construction
 
+// Coarse hierarchy k of every member at level depth d, in one launch: block q
+// fills level record recs[q] from its finer record by nearest-node injection.
 template <typename KT>
-void fill_hierarchy_k(BatchPlan& B, std::vector<KT*>& kh) {
-  for (int m = 0; m < B.count; ++m) {
-    const DevProblem& P = B.probs[m];
-    if (P.coef_kind != kDivk) continue;
-    const int r0 = B.lev0[m];
-    const long long n0 = B.levels[r0].g.n;
-    const int blocks = (int)std::min<long long>((n0 + 255) / 256, 148LL * 8);
-    k_convert<KT, double><<<blocks, 256, 0, B.stream>>>(n0, kh[r0], P.cd.k);
-    for (int l = 1; l < B.nlev[m]; ++l) {
-      const GridDev& gf = B.levels[r0 + l - 1].g;
-      const GridDev& gc = B.levels[r0 + l].g;
-      const int cb = (int)std::min<long long>((gc.n + 255) / 256, 148LL * 8);
-      k_inject<KT><<<cb, 256, 0, B.stream>>>(gf, gc, kh[r0 + l - 1], kh[r0 + l]);
-    }
+__global__ void kb_inject(const int* __restrict__ recs, const BLevel* __restrict__ lv) {
+  const BLevel& C = lv[recs[blockIdx.x]];
+  const BLevel& F = lv[C.prev];
+  const KT* kf = static_cast<const KT*>(F.kh);
+  KT* kc = static_cast<KT*>(const_cast<void*>(C.kh));
+  const GridDev& gc = C.g;
+  const GridDev& gf = F.g;
+  for (long long t = threadIdx.x; t < gc.n; t += blockDim.x) {
+    const int I = int(t % gc.nx);
+    const int J = int((t / gc.nx) % gc.ny);
+    const int K = int(t / gc.sxy);
+    const int fi = nearest_fine(I, gf.nx, gc.nx), fj = nearest_fine(J, gf.ny, gc.ny);
+    const int fk = gc.dim == 3 ? nearest_fine(K, gf.nz, gc.nz) : 0;
+    kc[t] = kf[((long long)fk * gf.ny + fj) * gf.nx + fi];
   }
+}
+
+template <typename KT>
+void fill_hierarchy_k(BatchPlan& B, KT* kh0, float* k32, const double* k64) {
+  const long long n = B.nodes;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  k_convert<KT, double><<<blocks, 256, 0, B.stream>>>(n, kh0, k64);
+  k_convert<float, double><<<blocks, 256, 0, B.stream>>>(n, k32, k64);
+  std::vector<std::vector<int>> by_depth(B.lmax);
+  for (size_t r = 0; r < B.levels.size(); ++r)
+    if (B.levels[r].level > 0 && B.levels[r].kind == kDivk) by_depth[B.levels[r].level].push_back((int)r);
+  std::vector<int> flat;
+  std::vector<size_t> start(B.lmax, 0);
+  for (int d = 1; d < B.lmax; ++d) {
+    start[d] = flat.size();
+    flat.insert(flat.end(), by_depth[d].begin(), by_depth[d].end());
+  }
+  if (flat.empty()) return;
+  Buf recs(sizeof(int) * flat.size(), B.stream);
+  PDEB_CUDA(cudaMemcpyAsync(recs.as<void>(), flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice,
+                            B.stream));
+  for (int d = 1; d < B.lmax; ++d)
+    if (!by_depth[d].empty())
+      kb_inject<KT><<<(unsigned)by_depth[d].size(), 256, 0, B.stream>>>(recs.as<int>() + start[d],
+                                                                           B.d_levels.as<BLevel>());
   PDEB_CUDA(cudaGetLastError());
+  PDEB_CUDA(cudaStreamSynchronize(B.stream));  // recs is released on return
 }
 
 void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pdeb200_batch_options* o) {
@@ -325,8 +353,7 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
   B.bf16 = o->bf16_coefficients != 0;
   B.use_graph = o->no_graph == 0;
   B.dev = o->device;
-  Context* base = get_context(o->device);
-  (void)base;
+  get_context(o->device);
   if (o->stream) {
     B.stream = static_cast<cudaStream_t>(o->stream);
   } else {
@@ -341,27 +368,23 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
   PDEB_CUDA(cudaMallocHost(&B.h_active, sizeof(int)));
   PDEB_CUDA(cudaMallocHost(&B.h_mem, sizeof(BMember) * count));
 
-  // members: validation, level-0 upload (faces, k), hierarchy geometry
+  // members: validation, geometry and faces of every level (host side)
   B.probs.resize(count);
   B.lev0.resize(count);
   B.nlev.resize(count);
   B.off.resize(count);
   B.mem_tmpl.assign(count, BMember{});
   long long n32 = 0, nkh = 0;
-  std::vector<long long> x_off, b_off, r_off, kh_off;  // per level record, in a32 / akh
-  std::vector<long long> k32_off(count, -1), p_off(count), q_off(count), e_off(count);
+  std::vector<long long> x_off, b_off, r_off, kh_off;  // per level record (kh: levels >= 1 only)
+  std::vector<long long> p_off(count), q_off(count), e_off(count);
   for (int m = 0; m < count; ++m) {
     const pdeb200_problem& hp = probs[m];
     if (hp.coef_kind != PDEB200_COEF_CONST && hp.coef_kind != PDEB200_COEF_DIVK)
       throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "batch members take COEF_CONST or COEF_DIVK"};
-    pdeb200_problem copy = hp;
-    copy.f = nullptr;
-    copy.u0 = nullptr;
-    upload_problem(&B.cx, &copy, &B.probs[m]);
+    describe_problem(&B.cx, &hp, &B.probs[m]);
     DevProblem& P = B.probs[m];
     B.off[m] = B.nodes;
     B.nodes += P.g.n;
-    // hierarchy geometry
     B.lev0[m] = (int)B.levels.size();
     BLevel L0{};
     L0.g = P.g;
@@ -412,7 +435,6 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
       throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "batch member too small for multigrid (needs a side of 5+ nodes)"};
     B.levels.back().coarsest = 1;
     B.lmax = std::max(B.lmax, B.nlev[m]);
-    // arena slots
     for (int l = 0; l < B.nlev[m]; ++l) {
       const long long n = B.levels[B.lev0[m] + l].g.n;
       x_off.push_back(n32);
@@ -421,89 +443,84 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
       n32 += pad(n);
       r_off.push_back(n32);
       n32 += pad(n);
-      if (P.coef_kind == kDivk) {
+      if (l > 0 && P.coef_kind == kDivk) {
         kh_off.push_back(nkh);
         nkh += pad(n);
       } else {
         kh_off.push_back(-1);
       }
     }
-    const long long n0 = P.g.n;
-    if (P.coef_kind == kDivk) {
-      k32_off[m] = n32;
-      n32 += pad(n0);
-    }
+    const long long n0 = pad(P.g.n);
     p_off[m] = n32;
-    n32 += pad(n0);
+    n32 += n0;
     q_off[m] = n32;
-    n32 += pad(n0);
+    n32 += n0;
     e_off[m] = n32;
-    n32 += pad(n0);
+    n32 += n0;
   }
-  // arenas: FP64 f | b | x (packed, member order), FP32 vectors, hierarchy k
-  B.a64 = Buf(sizeof(double) * 3 * (size_t)B.nodes, B.stream);
+  // arenas. FP64: f | b | x | k (packed in member order); FP32: k (packed),
+  // level vectors and p, q, e; hierarchy k: level 0 packed, then coarse levels.
+  const long long N = B.nodes;
+  B.a64 = Buf(sizeof(double) * 4 * (size_t)N, B.stream);
   B.f64 = B.a64.as<double>();
-  B.b64 = B.f64 + B.nodes;
-  B.x64 = B.b64 + B.nodes;
-  PDEB_CUDA(cudaMemsetAsync(B.a64.as<void>(), 0, sizeof(double) * 3 * (size_t)B.nodes, B.stream));
-  B.a32 = Buf(sizeof(float) * (size_t)n32, B.stream);
-  PDEB_CUDA(cudaMemsetAsync(B.a32.as<void>(), 0, sizeof(float) * (size_t)n32, B.stream));
-  const size_t khsz = B.bf16 ? sizeof(__nv_bfloat16) : sizeof(float);
-  if (nkh > 0) B.akh = Buf(khsz * (size_t)nkh, B.stream);
+  B.b64 = B.f64 + N;
+  B.x64 = B.b64 + N;
+  double* k64 = B.x64 + N;
+  PDEB_CUDA(cudaMemsetAsync(B.a64.as<void>(), 0, sizeof(double) * 4 * (size_t)N, B.stream));
+  B.a32 = Buf(sizeof(float) * (size_t)(n32 + N), B.stream);
+  PDEB_CUDA(cudaMemsetAsync(B.a32.as<void>(), 0, sizeof(float) * (size_t)(n32 + N), B.stream));
   float* a32 = B.a32.as<float>();
+  float* k32 = a32 + n32;
+  const size_t khsz = B.bf16 ? sizeof(__nv_bfloat16) : sizeof(float);
+  B.akh = Buf(khsz * (size_t)(N + nkh), B.stream);
   char* akh = B.akh.as<char>();
-  std::vector<float*> kh32(B.levels.size(), nullptr);
-  std::vector<__nv_bfloat16*> kh16(B.levels.size(), nullptr);
-  for (size_t r = 0; r < B.levels.size(); ++r) {
-    BLevel& L = B.levels[r];
-    L.x = a32 + x_off[r];
-    L.b = a32 + b_off[r];
-    L.r = a32 + r_off[r];
-    if (kh_off[r] >= 0) {
-      void* ptr = akh + khsz * (size_t)kh_off[r];
-      L.kh = ptr;
-      kh32[r] = static_cast<float*>(ptr);
-      kh16[r] = static_cast<__nv_bfloat16*>(ptr);
-    } else {
-      L.kh = nullptr;
+  for (int m = 0; m < count; ++m) {
+    for (int l = 0; l < B.nlev[m]; ++l) {
+      const int r = B.lev0[m] + l;
+      BLevel& L = B.levels[r];
+      L.x = a32 + x_off[r];
+      L.b = a32 + b_off[r];
+      L.r = a32 + r_off[r];
+      if (L.kind != kDivk)
+        L.kh = nullptr;
+      else if (l == 0)
+        L.kh = akh + khsz * (size_t)B.off[m];
+      else
+        L.kh = akh + khsz * (size_t)(N + kh_off[r]);
     }
   }
-  // right-hand sides and member records
+  // inputs into the packed FP64 arena (one copy per array and member)
   for (int m = 0; m < count; ++m) {
     const pdeb200_problem& hp = probs[m];
     const DevProblem& P = B.probs[m];
     const long long n0 = P.g.n;
+    const cudaMemcpyKind kind = hp.mem_space == PDEB200_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     double* fm = B.f64 + B.off[m];
     if (hp.f) {
-      const cudaMemcpyKind kind =
-          hp.mem_space == PDEB200_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
       PDEB_CUDA(cudaMemcpyAsync(fm, hp.f, sizeof(double) * n0, kind, B.stream));
     } else if (hp.f_const != 0.0) {
       const int blocks = (int)std::min<long long>((n0 + 255) / 256, 148LL * 8);
       k_fill<double><<<blocks, 256, 0, B.stream>>>(n0, fm, hp.f_const, nullptr);
     }
+    if (P.coef_kind == kDivk) PDEB_CUDA(cudaMemcpyAsync(k64 + B.off[m], hp.k, sizeof(double) * n0, kind, B.stream));
     BMember& M = B.mem_tmpl[m];
     M.level0 = B.lev0[m];
     M.x64 = B.x64 + B.off[m];
     M.b64 = B.b64 + B.off[m];
     M.f64 = fm;
-    M.k64 = P.coef_kind == kDivk ? P.cd.k : nullptr;
-    M.k32 = k32_off[m] >= 0 ? a32 + k32_off[m] : nullptr;
+    M.k64 = P.coef_kind == kDivk ? k64 + B.off[m] : nullptr;
+    M.k32 = P.coef_kind == kDivk ? k32 + B.off[m] : nullptr;
     M.p = a32 + p_off[m];
     M.q = a32 + q_off[m];
     M.e = a32 + e_off[m];
-    if (M.k32) {
-      const int blocks = (int)std::min<long long>((n0 + 255) / 256, 148LL * 8);
-      k_convert<float, double><<<blocks, 256, 0, B.stream>>>(n0, a32 + k32_off[m], P.cd.k);
-    }
   }
-  if (B.bf16)
-    fill_hierarchy_k<__nv_bfloat16>(B, kh16);
-  else
-    fill_hierarchy_k<float>(B, kh32);
   B.d_levels = Buf(sizeof(BLevel) * B.levels.size(), B.stream);
   PDEB_CUDA(cudaMemcpyAsync(B.d_levels.as<void>(), B.levels.data(), sizeof(BLevel) * B.levels.size(),
                             cudaMemcpyHostToDevice, B.stream));
+  if (B.bf16)
+    fill_hierarchy_k<__nv_bfloat16>(B, reinterpret_cast<__nv_bfloat16*>(akh), k32, k64);
+  else
+    fill_hierarchy_k<float>(B, reinterpret_cast<float*>(akh), k32, k64);
   B.d_mem = Buf(sizeof(BMember) * count, B.stream);
   B.d_active = Buf(sizeof(int), B.stream);
   PDEB_CUDA(cudaStreamSynchronize(B.stream));

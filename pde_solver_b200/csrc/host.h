@@ -203,6 +203,9 @@ struct DevProblem {
 
 // Validates and uploads; host arrays of the problem are copied on ctx->stream.
 void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* out);
+// Validation, geometry, faces and coefficient scalars only: f, u0, k and
+// nodal stay unset (the caller places them).
+void describe_problem(Context* ctx, const pdeb200_problem* p, DevProblem* out);
 
 // Builds the face parameters of `g` for spacing (dx,dy,dz) from the host face
 // descriptions; arrays are sampled with `stride` (1 on the finest level, 2^l

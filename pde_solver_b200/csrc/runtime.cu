@@ -275,6 +275,21 @@ void build_faces(Context* ctx, const pdeb200_problem* p, int nx, int ny, int nz,
 }
 
 void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
+  describe_problem(ctx, p, P);
+  const long long n = P->g.n;
+  auto take = [&](const double* ptr, size_t count) -> const double* {
+    if (!ptr) return nullptr;
+    if (P->device_inputs) return ptr;
+    P->owned.push_back(upload(ctx, ptr, sizeof(double) * count));
+    return P->owned.back().as<double>();
+  };
+  P->f = take(p->f, n);
+  P->u0 = take(p->u0, n);
+  if (p->coef_kind == PDEB200_COEF_DIVK) P->cd.k = take(p->k, n);
+  if (p->coef_kind == PDEB200_COEF_NODAL) P->cn.nodal = take(p->nodal, 7 * n);
+}
+
+void describe_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
   if (!p) throw StatusFailure{PDEB200_ERR_INVALID, "null problem"};
   const int dim = p->nz > 1 ? 3 : 2;
   if (p->nx < 3 || p->ny < 3 || (dim == 3 && p->nz < 3))
@@ -309,21 +324,13 @@ void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
   P->f_const = p->f_const;
   P->device_inputs = p->mem_space == PDEB200_MEM_DEVICE;
   build_faces(ctx, p, g.nx, g.ny, g.nz, P->dx, P->dy, P->dz, 1, &g, &P->owned);
-  auto take = [&](const double* ptr, size_t count) -> const double* {
-    if (!ptr) return nullptr;
-    if (P->device_inputs) return ptr;
-    P->owned.push_back(upload(ctx, ptr, sizeof(double) * count));
-    return P->owned.back().as<double>();
-  };
-  P->f = take(p->f, n);
-  P->u0 = take(p->u0, n);
   switch (p->coef_kind) {
     case PDEB200_COEF_CONST:
       P->cc = make_const(p->a, p->b, p->az, p->c, p->d, p->dz, p->e, P->dx, P->dy, P->dz, dim);
       break;
     case PDEB200_COEF_DIVK: {
       if (!p->k) throw StatusFailure{PDEB200_ERR_INVALID, "COEF_DIVK needs k"};
-      P->cd.k = take(p->k, n);
+      P->cd.k = nullptr;
       P->cd.ihx2 = 1.0 / (P->dx * P->dx);
       P->cd.ihy2 = 1.0 / (P->dy * P->dy);
       P->cd.ihz2 = dim == 3 ? 1.0 / (P->dz * P->dz) : 0.0;
@@ -335,7 +342,7 @@ void upload_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
     }
     case PDEB200_COEF_NODAL: {
       if (!p->nodal) throw StatusFailure{PDEB200_ERR_INVALID, "COEF_NODAL needs nodal arrays"};
-      P->cn.nodal = take(p->nodal, 7 * n);
+      P->cn.nodal = nullptr;
       P->cn.n = n;
       P->cn.dx2 = P->dx * P->dx;
       P->cn.dy2 = P->dy * P->dy;
