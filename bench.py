@@ -310,23 +310,18 @@ def main():
     from pde_solver_b200 import abi, synthetic
     from pde_solver_b200.problem import default_options
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
+    from pde_solver_b200 import replicas
+
+    world, rank, local = replicas.rank_env()
     if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = replicas.init("nccl", timeout_s=600)
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     lib = abi.load()
 
     n = args.n
-    prob = synthetic.varcoef_poisson_3d(n, seed=SEED + rank)
+    prob = synthetic.varcoef_poisson_3d(n, seed=replicas.replica_seed(SEED, rank))
     N = prob.n
     opt = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400, device=local)
     stream = torch.cuda.current_stream(device)
@@ -375,11 +370,8 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = replicas.max_over_ranks(ms, dist, device)
+    value = replicas.aggregate_rate(world, args.steps, ms)
 
     # ---- end to end through the same C-ABI call with pinned host buffers
     k_host = torch.from_numpy(prob.k).pin_memory()
@@ -409,11 +401,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms_e2e = e2.elapsed_time(e3)
-    if dist is not None:
-        t = torch.tensor([ms_e2e], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * args.steps / (ms_e2e / 1e3)
+    ms_e2e = replicas.max_over_ranks(ms_e2e, dist, device)
+    e2e_value = replicas.aggregate_rate(world, args.steps, ms_e2e)
     ok_host = np.allclose(out_host.numpy(), out_dev.cpu().numpy(), rtol=0, atol=1e-12 * float(out_dev.abs().max()))
 
     # ---- live per-kernel roofline (events around each finest-level launch)
