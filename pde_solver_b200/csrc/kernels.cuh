@@ -915,4 +915,169 @@ __global__ void k_coarse_solve_smem(GridDev g, Coef cf, const TB* __restrict__ b
   for (int t = tid; t < n; t += blockDim.x) x[t] = sx[t];
 }
 
+// ------------------------------------------------------- single-block tail
+
+// The small levels of a V-cycle in one launch. Levels [0, nlev) of `lv` are
+// the hierarchy's levels from the first small one down to the coarsest; the
+// block runs, with a barrier between phases, exactly the sequence the
+// per-level launches run: zero fill and `pre` red-black sweeps, residual,
+// full-weighting restriction and boundary fold, recursion, trilinear
+// prolongation-add of the extended correction and `post` sweeps (colour order
+// reversed), and `coarse_iters` sweeps from zero on the coarsest level. The
+// arithmetic of every node update is that of k_rbgs / k_residual_folded /
+// full_weight / k_restrict_fold / k_prolong_add. rhs0 is the right-hand side of
+// level 0 of the tail; the result is left in lv[0].x.
+template <class Coef, typename T>
+struct TailLevel {
+  GridDev g;
+  Coef cf;
+  T* x;
+  T* b;
+  T* r;
+};
+
+constexpr int kTailThreads = 512;
+constexpr int kTailMaxLevels = 8;
+
+template <class Coef, typename T>
+__device__ __forceinline__ void tail_decode(const GridDev& g, int t, int& i, int& j, int& k) {
+  const int ni = g.nx - 2, nj = g.ny - 2;
+  i = 1 + t % ni;
+  j = 1 + (t / ni) % nj;
+  k = (g.dim == 3 ? 1 : 0) + t / (ni * nj);
+}
+
+template <class Coef, typename T>
+__device__ void tail_sweeps(const TailLevel<Coef, T>& L, const T* b, int sweeps, int first) {
+  const GridDev& g = L.g;
+  const int total = (g.nx - 2) * (g.ny - 2) * (g.dim == 3 ? g.nz - 2 : 1);
+  T* x = L.x;
+  for (int s = 0; s < sweeps; ++s)
+    for (int half = 0; half < 2; ++half) {
+      const int color = first ^ half;
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int i, j, k;
+        tail_decode<Coef, T>(g, t, i, j, k);
+        if (((i + j + k) & 1) != color) continue;
+        const long long id = ((long long)k * g.ny + j) * g.nx + i;
+        Stencil<T> st = L.cf.template at<T>(g, id);
+        fold_faces<T>(g, i, j, k, st, nullptr);
+        const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+        const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+        x[id] = (T(b[id]) - nb_sum<T>(st, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / st.c;
+      }
+      __syncthreads();
+    }
+}
+
+template <class Coef, typename T>
+__device__ void tail_zero(const TailLevel<Coef, T>& L) {
+  for (long long t = threadIdx.x; t < L.g.n; t += blockDim.x) L.x[t] = T(0);
+  __syncthreads();
+}
+
+template <class Coef, typename T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel<Coef, T>* __restrict__ lv, int nlev,
+                                                               const T* __restrict__ rhs0, int pre, int post,
+                                                               int coarse_iters, int fold, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  // down: smooth, residual, restrict
+  for (int l = 0; l + 1 < nlev; ++l) {
+    const TailLevel<Coef, T>& L = lv[l];
+    const T* b = l == 0 ? rhs0 : L.b;
+    const GridDev& g = L.g;
+    tail_zero(L);
+    tail_sweeps(L, b, pre, 0);
+    const int total = (g.nx - 2) * (g.ny - 2) * (g.dim == 3 ? g.nz - 2 : 1);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      int i, j, k;
+      tail_decode<Coef, T>(g, t, i, j, k);
+      const long long id = ((long long)k * g.ny + j) * g.nx + i;
+      Stencil<T> s = L.cf.template at<T>(g, id);
+      fold_faces<T>(g, i, j, k, s, nullptr);
+      const T* x = L.x;
+      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+      const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+      L.r[id] = T(b[id]) - (s.c * x[id] + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm,
+                                                    g.dim));
+    }
+    __syncthreads();
+    const TailLevel<Coef, T>& C = lv[l + 1];
+    const GridDev& gc = C.g;
+    for (long long t = threadIdx.x; t < gc.n; t += blockDim.x) {
+      const int I = int(t % gc.nx), J = int((t / gc.nx) % gc.ny), K = int(t / gc.sxy);
+      C.b[t] = T(full_weight<T>(g, gc, L.r, I, J, K));
+    }
+    __syncthreads();
+    if (fold) {
+      const int ctotal = (gc.nx - 2) * (gc.ny - 2) * (gc.dim == 3 ? gc.nz - 2 : 1);
+      // each interior coarse node next to a face gathers the boundary values
+      // whose closure chain ends at it; writes go to interior nodes only and
+      // reads to boundary nodes only, so one pass is race free
+      for (int t = threadIdx.x; t < ctotal; t += blockDim.x) {
+        int I, J, K;
+        tail_decode<Coef, T>(gc, t, I, J, K);
+        const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
+        const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
+        const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+        if (dxl == 0 && dxh == 0 && dyl == 0 && dyh == 0 && dzl == 0 && dzh == 0) continue;
+        double acc = 0.0;
+        for (int dk = dzl; dk <= dzh; ++dk)
+          for (int dj = dyl; dj <= dyh; ++dj)
+            for (int di = dxl; di <= dxh; ++di) {
+              if (di == 0 && dj == 0 && dk == 0) continue;
+              int ci = I + di, cj = J + dj, ck = K + dk;
+              const double coef = ext_chain(gc, ci, cj, ck);
+              if (coef != 0.0 && ci == I && cj == J && ck == K)
+                acc += coef * double(C.b[cidx(gc, I + di, J + dj, K + dk)]);
+            }
+        if (acc != 0.0) {
+          const long long id = cidx(gc, I, J, K);
+          C.b[id] = T(double(C.b[id]) + acc);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // coarsest level: sweeps from zero
+  {
+    const TailLevel<Coef, T>& L = lv[nlev - 1];
+    tail_zero(L);
+    tail_sweeps(L, nlev == 1 ? rhs0 : L.b, coarse_iters, 0);
+  }
+  // up: prolong-add, post-smooth
+  for (int l = nlev - 2; l >= 0; --l) {
+    const TailLevel<Coef, T>& F = lv[l];
+    const TailLevel<Coef, T>& C = lv[l + 1];
+    const GridDev& gf = F.g;
+    const GridDev& gc = C.g;
+    const int xmode = map_mode(gf.nx, gc.nx), ymode = map_mode(gf.ny, gc.ny);
+    const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
+    const int total = (gf.nx - 2) * (gf.ny - 2) * (gf.dim == 3 ? gf.nz - 2 : 1);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      int i, j, k;
+      tail_decode<Coef, T>(gf, t, i, j, k);
+      int I0, J0, K0 = 0;
+      double tx, ty, tz = 0.0;
+      coarse_pos(i, gf.nx, gc.nx, xmode, I0, tx);
+      coarse_pos(j, gf.ny, gc.ny, ymode, J0, ty);
+      if (gf.dim == 3) coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+      const int I1 = tx != 0.0 ? I0 + 1 : I0, J1 = ty != 0.0 ? J0 + 1 : J0;
+      const int K1 = tz != 0.0 ? K0 + 1 : K0;
+      const double c000 = ext_value(gc, C.x, I0, J0, K0), c100 = ext_value(gc, C.x, I1, J0, K0);
+      const double c010 = ext_value(gc, C.x, I0, J1, K0), c110 = ext_value(gc, C.x, I1, J1, K0);
+      const double c001 = ext_value(gc, C.x, I0, J0, K1), c101 = ext_value(gc, C.x, I1, J0, K1);
+      const double c011 = ext_value(gc, C.x, I0, J1, K1), c111 = ext_value(gc, C.x, I1, J1, K1);
+      const double x00 = (1.0 - tx) * c000 + tx * c100, x10 = (1.0 - tx) * c010 + tx * c110;
+      const double x01 = (1.0 - tx) * c001 + tx * c101, x11 = (1.0 - tx) * c011 + tx * c111;
+      const double y0 = (1.0 - ty) * x00 + ty * x10, y1 = (1.0 - ty) * x01 + ty * x11;
+      const double v = (1.0 - tz) * y0 + tz * y1;
+      const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
+      F.x[id] = T(double(F.x[id]) + v);
+    }
+    __syncthreads();
+    tail_sweeps(F, l == 0 ? rhs0 : F.b, post, 1);
+  }
+}
+
 }  // namespace pdeb

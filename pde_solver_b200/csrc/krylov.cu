@@ -568,7 +568,21 @@ pdeb200_status mg_bicgstab_core(Context* ctx, HierT& H, const GridDev& g, const 
     k_bi_r<T, PostBiResid><<<nb, 256, 0, ctx->stream>>>(n, r, s, t, ctx->slot(), PostBiResid{C, 1}, C);
     ctx->count(12);
   };
-  pdeb200_status st = drive(ctx, o, max_iter + 1, iterate, false);
+  // iterations after the first are identical: replay them as a graph
+  IterGraph graph;
+  int graphed = -1;
+  auto step = [&](int it) {
+    if (it == 0) {
+      iterate(0);
+      return;
+    }
+    if (graphed < 0) graphed = graph.capture(ctx, [&](int) { iterate(1); }) ? 1 : 0;
+    if (graphed)
+      graph.launch(ctx);
+    else
+      iterate(it);
+  };
+  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
   const Ctl c = ctl_poll(ctx);
   *iters = c.iter;
   return st;
@@ -688,7 +702,15 @@ pdeb200_status mg_pcg_core(Context* ctx, HierT& H, const GridDev& g, const Coef&
     k_cg_p<T><<<nb, 256, 0, ctx->stream>>>(n, p, z, C, 0);
     ctx->count(4);
   };
-  pdeb200_status st = drive(ctx, o, max_iter + 1, iterate, false);
+  IterGraph graph;
+  const bool graphed = graph.capture(ctx, iterate);
+  auto step = [&](int it) {
+    if (graphed)
+      graph.launch(ctx);
+    else
+      iterate(it);
+  };
+  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
   const Ctl c = ctl_poll(ctx);
   *iters = c.iter;
   return st;

@@ -165,7 +165,15 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
     }
     ctx->count(2);
   };
-  pdeb200_status st = drive(ctx, o, max_iter + 1, iterate, false);
+  IterGraph graph;
+  const bool graphed = graph.capture(ctx, iterate);
+  auto step = [&](int it) {
+    if (graphed)
+      graph.launch(ctx);
+    else
+      iterate(it);
+  };
+  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
   const Ctl c = ctl_poll(ctx);
   if (rep) {
     rep->iterations = c.iter;

@@ -177,6 +177,66 @@ pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& 
   }
 }
 
+// One solver iteration captured once as a CUDA graph and replayed. `iterate`
+// must only enqueue kernels on ctx->stream (they all read the device control
+// block, so a replay after convergence is a no-op like a direct launch). The
+// capture runs on the context's own stream, since the caller's stream may be
+// the legacy default stream, which cannot be captured; replays go to
+// ctx->stream. Off while per-kernel profiling is on or PDEB200_NO_GRAPH is set.
+struct IterGraph {
+  cudaGraphExec_t exec = nullptr;
+  long long launches_per_iter = 0;
+  IterGraph() = default;
+  IterGraph(const IterGraph&) = delete;
+  IterGraph& operator=(const IterGraph&) = delete;
+  ~IterGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  template <class It>
+  bool capture(Context* ctx, It&& iterate) {
+    if (ctx->prof || std::getenv("PDEB200_NO_GRAPH") != nullptr) return false;
+    cudaStream_t saved = ctx->stream;
+    const long long before = ctx->launches;
+    ctx->stream = ctx->own_stream;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      ctx->stream = saved;
+      cudaGetLastError();
+      return false;
+    }
+    cudaGraph_t g = nullptr;
+    try {
+      iterate(0);
+    } catch (...) {
+      cudaStreamEndCapture(ctx->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      ctx->stream = saved;
+      cudaGetLastError();
+      throw;
+    }
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->stream = saved;
+    launches_per_iter = ctx->launches - before;
+    ctx->launches = before;
+    if (e != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return false;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      exec = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    return true;
+  }
+  void launch(Context* ctx) {
+    PDEB_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    ctx->launches += launches_per_iter;
+  }
+};
+
 inline void fill_boundary(Context* ctx, const GridDev& g, double* u, const Ctl* ctl, bool dirichlet_last = true) {
   const long long faces = 2LL * g.ny * g.nz + 2LL * g.nx * g.nz + (g.dim == 3 ? 2LL * g.nx * g.ny : 0);
   const int blocks = vec_blocks(faces, ctx);
@@ -384,6 +444,11 @@ struct Hierarchy {
     return p;
   }
 
+  // Levels from tail_l0 down run as one single-block launch (k_tail_vcycle).
+  static constexpr long long kTailMaxNodes = 1100;
+  int tail_l0 = -1;
+  TailLevel<Coef, T>* d_tail = nullptr;
+
   bool coarse_in_smem(const Level& L) const {
     const long long interior = (long long)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.dim == 3 ? L.g.nz - 2 : 1);
     return L.g.n <= kCoarseMaxNodes && interior <= kCoarseMaxInterior;
@@ -428,6 +493,26 @@ struct Hierarchy {
       c.b = alloc(ctx, c.g.n);
       c.r = alloc(ctx, c.g.n);
       levels.push_back(c);
+    }
+    // single-block tail: the first level small enough, with at most
+    // kTailMaxLevels levels below it (colour-pass form only)
+    tail_l0 = -1;
+    if (!fused && std::getenv("PDEB200_NO_TAIL") == nullptr) {
+      for (size_t l = 0; l < levels.size(); ++l)
+        if (levels[l].g.n <= kTailMaxNodes && (int)(levels.size() - l) <= kTailMaxLevels) {
+          tail_l0 = (int)l;
+          break;
+        }
+    }
+    if (tail_l0 >= 0) {
+      std::vector<TailLevel<Coef, T>> tl;
+      for (size_t l = tail_l0; l < levels.size(); ++l)
+        tl.push_back(TailLevel<Coef, T>{levels[l].g, levels[l].cf, levels[l].xa, levels[l].b, levels[l].r});
+      owned.emplace_back(sizeof(TailLevel<Coef, T>) * tl.size(), ctx->stream);
+      d_tail = owned.back().template as<TailLevel<Coef, T>>();
+      PDEB_CUDA(cudaMemcpyAsync(d_tail, tl.data(), sizeof(TailLevel<Coef, T>) * tl.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+      PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
     }
     // result buffer of each level after a V-cycle (fixed, so launches can be captured):
     // the first sweep from zero writes xa, every later sweep flips the buffer
@@ -490,6 +575,13 @@ struct Hierarchy {
     Level& L = levels[l];
     const T* b = l == 0 ? rhs0 : L.b;
     const double dofs = interior_dofs(L.g);
+    if (l == tail_l0) {
+      ProfScope ps(ctx, "tail_vcycle", l, 0.0);
+      k_tail_vcycle<Coef, T><<<1, kTailThreads, 0, ctx->stream>>>(d_tail, (int)levels.size() - l, b, pre, post,
+                                                                    coarse_iters, needs_fold ? 1 : 0, ctl);
+      ctx->count();
+      return;
+    }
     if (l == (int)levels.size() - 1) {
       if (coarse_in_smem(L)) {
         ProfScope ps(ctx, "coarse_solve", l, 0.0);
