@@ -95,6 +95,9 @@ pdeb200_status pdeb200_batch_solve(pdeb200_batch* b, double tol, pdeb200_report*
 /* Copies every member's solution (boundary nodes included) into `out_packed`. */
 pdeb200_status pdeb200_batch_read(pdeb200_batch* b, double* out_packed, int32_t mem_space);
 
+/* Copies one member's solution (nx*ny*nz values) into `out` (host or device). */
+pdeb200_status pdeb200_batch_read_member(pdeb200_batch* b, int32_t member, double* out, int32_t mem_space);
+
 /* Options in effect (after defaults and autotuning). */
 pdeb200_status pdeb200_batch_get_options(const pdeb200_batch* b, pdeb200_batch_options* opt);
 

@@ -50,7 +50,10 @@ typedef struct {
 typedef struct {
   int32_t kind;              /* pdeb200_request_kind */
   int32_t steps;             /* HEAT: forward-Euler steps */
-  const pdeb200_problem* problem; /* POISSON, HEAT (host arrays; copied at submit) */
+  /* POISSON, HEAT. Host arrays (mem_space HOST) are copied at submit; device
+   * arrays (mem_space DEVICE) are used in place and must stay valid until the
+   * request completes, and `out` is then a device pointer. */
+  const pdeb200_problem* problem;
   double tol;                /* POISSON: relative residual; 0 = 1e-10 */
   double t_start, dt;        /* HEAT */
   /* PROJECTION (host arrays, copied at submit; nz <= 1 is 2D) */

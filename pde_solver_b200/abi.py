@@ -340,6 +340,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_batch_solve.argtypes = [C.c_void_p, C.c_double, P(Report), P(BatchStats)]
     lib.pdeb200_batch_read.restype = C.c_int32
     lib.pdeb200_batch_read.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.pdeb200_batch_read_member.restype = C.c_int32
+    lib.pdeb200_batch_read_member.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
     lib.pdeb200_batch_get_options.restype = C.c_int32
     lib.pdeb200_batch_get_options.argtypes = [C.c_void_p, P(BatchOptions)]
     lib.pdeb200_batch_destroy.restype = None

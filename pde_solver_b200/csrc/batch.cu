@@ -834,6 +834,21 @@ pdeb200_status pdeb200_batch_read(pdeb200_batch* b, double* out, int32_t mem_spa
   return PDEB200_OK;
 }
 
+pdeb200_status pdeb200_batch_read_member(pdeb200_batch* b, int32_t member, double* out, int32_t mem_space) {
+  using namespace pdeb;
+  if (!b || !out || member < 0 || member >= b->plan.count) return PDEB200_ERR_INVALID;
+  BatchPlan& B = b->plan;
+  const cudaMemcpyKind kind = mem_space == PDEB200_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t n = (size_t)B.probs[member].g.n;
+  if (cudaSetDevice(B.dev) != cudaSuccess ||
+      cudaMemcpyAsync(out, B.x64 + B.off[member], sizeof(double) * n, kind, B.stream) != cudaSuccess ||
+      cudaStreamSynchronize(B.stream) != cudaSuccess) {
+    cudaGetLastError();
+    return PDEB200_ERR_CUDA;
+  }
+  return PDEB200_OK;
+}
+
 pdeb200_status pdeb200_batch_get_options(const pdeb200_batch* b, pdeb200_batch_options* o) {
   if (!b || !o) return PDEB200_ERR_INVALID;
   const pdeb::BatchPlan& B = b->plan;

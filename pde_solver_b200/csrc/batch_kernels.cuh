@@ -544,11 +544,29 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
   const GridDev& gc = C.g;
   const float* __restrict__ rf = F.r;
   float* __restrict__ bc = C.b;
+  const bool zmarch = gc.dim != 3 || map_mode(F.g.nz, gc.nz) <= 1;
+  const bool zsame = gc.dim == 3 && gc.nz == F.g.nz;
   tile_columns(T, [&](int I, int J) {
     const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
     const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
+    FwColumn<float> col;
+    col.init(F.g, gc, rf, I, J);
+    // nested z: fine plane 2K+1 feeds coarse planes K and K+1 (sum kept)
+    double below = zmarch && gc.dim == 3 && !zsame ? col.plane(2 * T.z0 - 1) : 0.0;
     for (int K = T.z0; K < T.z1; ++K) {
-      double acc = full_weight<float>(F.g, gc, rf, I, J, K);
+      double acc;
+      if (!zmarch) {
+        acc = full_weight<float>(F.g, gc, rf, I, J, K);
+      } else if (gc.dim != 3) {
+        acc = col.plane(0);
+      } else if (zsame) {
+        acc = col.plane(K);
+      } else {
+        const double mid = col.plane(2 * K);
+        const double above = 2 * K + 1 <= F.g.nz - 1 ? col.plane(2 * K + 1) : 0.0;
+        acc = 0.25 * below + 0.5 * mid + 0.25 * above;
+        below = above;
+      }
       const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
       if (dxl | dxh | dyl | dyh | dzl | dzh) {
         for (int dk = dzl; dk <= dzh; ++dk)
@@ -591,38 +609,43 @@ __global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict_
     coarse_pos(j, gf.ny, gc.ny, ymode, J0, ty);
     const int I1 = tx != 0.0 ? I0 + 1 : I0, J1 = ty != 0.0 ? J0 + 1 : J0;
     const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
-    for (int k = T.z0; k < T.z1; ++k) {
-      int K0 = 0, K1 = 0;
-      double tz = 0.0;
-      if (gf.dim == 3) {
-        coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
-        K1 = tz != 0.0 ? K0 + 1 : K0;
-      }
-      double c000, c100, c010, c110, c001, c101, c011, c111;
-      if (!xy_edge && !(gf.dim == 3 && (K0 == 0 || K1 == gc.nz - 1))) {
-        const long long a0 = (long long)K0 * gc.sxy, a1 = (long long)K1 * gc.sxy;
+    // bilinear x-y value on coarse plane K, kept for the fine planes it feeds
+    auto bilinear = [&](int K) -> double {
+      double c00, c10, c01, c11;
+      if (!xy_edge && !(gf.dim == 3 && (K == 0 || K == gc.nz - 1))) {
+        const long long a = (long long)K * gc.sxy;
         const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
-        c000 = double(xc[a0 + r0 + I0]);
-        c100 = double(xc[a0 + r0 + I1]);
-        c010 = double(xc[a0 + r1 + I0]);
-        c110 = double(xc[a0 + r1 + I1]);
-        c001 = double(xc[a1 + r0 + I0]);
-        c101 = double(xc[a1 + r0 + I1]);
-        c011 = double(xc[a1 + r1 + I0]);
-        c111 = double(xc[a1 + r1 + I1]);
+        c00 = double(xc[a + r0 + I0]);
+        c10 = double(xc[a + r0 + I1]);
+        c01 = double(xc[a + r1 + I0]);
+        c11 = double(xc[a + r1 + I1]);
       } else {
-        c000 = ext_value(gc, xc, I0, J0, K0);
-        c100 = ext_value(gc, xc, I1, J0, K0);
-        c010 = ext_value(gc, xc, I0, J1, K0);
-        c110 = ext_value(gc, xc, I1, J1, K0);
-        c001 = ext_value(gc, xc, I0, J0, K1);
-        c101 = ext_value(gc, xc, I1, J0, K1);
-        c011 = ext_value(gc, xc, I0, J1, K1);
-        c111 = ext_value(gc, xc, I1, J1, K1);
+        c00 = ext_value(gc, xc, I0, J0, K);
+        c10 = ext_value(gc, xc, I1, J0, K);
+        c01 = ext_value(gc, xc, I0, J1, K);
+        c11 = ext_value(gc, xc, I1, J1, K);
       }
-      const double x00 = (1.0 - tx) * c000 + tx * c100, x10 = (1.0 - tx) * c010 + tx * c110;
-      const double x01 = (1.0 - tx) * c001 + tx * c101, x11 = (1.0 - tx) * c011 + tx * c111;
-      const double y0 = (1.0 - ty) * x00 + ty * x10, y1 = (1.0 - ty) * x01 + ty * x11;
+      const double x0 = (1.0 - tx) * c00 + tx * c10, x1 = (1.0 - tx) * c01 + tx * c11;
+      return (1.0 - ty) * x0 + ty * x1;
+    };
+    int ka = -1, kb = -1;
+    double va = 0.0, vb = 0.0;
+    auto at = [&](int K) -> double {
+      if (K == ka) return va;
+      if (K == kb) return vb;
+      const double v = bilinear(K);
+      ka = kb;
+      va = vb;
+      kb = K;
+      vb = v;
+      return v;
+    };
+    for (int k = T.z0; k < T.z1; ++k) {
+      int K0 = 0;
+      double tz = 0.0;
+      if (gf.dim == 3) coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+      const double y0 = at(K0);
+      const double y1 = tz != 0.0 ? at(K0 + 1) : y0;
       const double v = (1.0 - tz) * y0 + tz * y1;
       const long long id = bid(gf, i, j, k);
       xf[id] = float(double(xf[id]) + v);

@@ -224,6 +224,9 @@ dim3 stencil_grid_full(const GridDev& g, int zchunk = 16);
 dim3 stencil_grid_auto(const GridDev& g);
 // launch shape of the fused red-black sweep (64 x 8 column tiles)
 dim3 fused_grid(const GridDev& g);
+// launch shape of the staged single-pass sweep (32 x 8 column tiles, z chunks
+// for about four resident blocks per SM over two waves)
+dim3 sweep_grid(const GridDev& g);
 inline int vec_blocks(long long n, const Context* ctx) {
   long long b = (n + 255) / 256;
   long long cap = (long long)ctx->num_sms * 8;

@@ -817,6 +817,132 @@ __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc
   }
 }
 
+// z-marching transfer kernels for level pairs whose z map is the identity or
+// nested 2:1 (every odd side, and every 2D grid). One thread per column:
+// restriction sums each fine plane's x-y weights once and shares the plane
+// sum between the two coarse planes it feeds; prolongation evaluates the
+// bilinear x-y interpolation once per coarse plane and reuses it for the 2-3
+// fine planes it feeds (same expressions as k_prolong_add, so the same bits).
+__device__ __forceinline__ bool z_marchable(const GridDev& gf, const GridDev& gc) {
+  return gf.dim != 3 || map_mode(gf.nz, gc.nz) <= 1;
+}
+
+// Full weighting of one coarse column (I, J): the x-y weights once, then the
+// weighted sum of any fine plane.
+template <typename T>
+struct FwColumn {
+  const T* rf;
+  int nx, ny, ix0, iy0;
+  double wx[4], wy[4];
+  __device__ __forceinline__ void init(const GridDev& gf, const GridDev& gc, const T* r, int I, int J) {
+    rf = r;
+    nx = gf.nx;
+    ny = gf.ny;
+    restrict_weights(I, gf.nx, gc.nx, map_mode(gf.nx, gc.nx), ix0, wx);
+    restrict_weights(J, gf.ny, gc.ny, map_mode(gf.ny, gc.ny), iy0, wy);
+  }
+  __device__ __forceinline__ double plane(int kf) const {
+    double acc = 0.0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (wy[b] == 0.0) continue;
+      const T* row = rf + ((long long)kf * ny + clampi(iy0 + b, ny - 1)) * nx;
+      double rs = 0.0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (wx[a] != 0.0) rs += wx[a] * double(row[clampi(ix0 + a, nx - 1)]);
+      acc += wy[b] * rs;
+    }
+    return acc;
+  }
+};
+
+template <typename T, typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_restrict_march(GridDev gf, GridDev gc, const T* __restrict__ rf,
+                                                             TC* __restrict__ bc, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int I = blockIdx.x * kBx + threadIdx.x;
+  const int J = blockIdx.y * kBy + threadIdx.y;
+  if (I >= gc.nx || J >= gc.ny) return;
+  const int chunk = (gc.nz + gridDim.z - 1) / gridDim.z;
+  const int K0 = blockIdx.z * chunk, K1 = min(gc.nz, K0 + chunk);
+  FwColumn<T> col;
+  col.init(gf, gc, rf, I, J);
+  auto plane = [&](int kf) -> double { return col.plane(kf); };
+  const long long cxy = (long long)J * gc.nx + I;
+  if (gc.dim != 3 || gc.nz == gf.nz) {
+    for (int K = K0; K < K1; ++K) bc[(long long)K * gc.sxy + cxy] = TC(plane(K));
+    return;
+  }
+  // nested 2:1 in z: coarse K takes fine planes 2K-1, 2K, 2K+1 with 1/4, 1/2, 1/4
+  double below = 2 * K0 - 1 >= 0 ? plane(2 * K0 - 1) : 0.0;
+  for (int K = K0; K < K1; ++K) {
+    const double mid = plane(2 * K);
+    const double above = 2 * K + 1 <= gf.nz - 1 ? plane(2 * K + 1) : 0.0;
+    bc[(long long)K * gc.sxy + cxy] = TC(0.25 * below + 0.5 * mid + 0.25 * above);
+    below = above;
+  }
+}
+
+template <typename T, typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_prolong_march(GridDev gf, GridDev gc, const TC* __restrict__ xc,
+                                                            T* __restrict__ xf, const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(gf, k0, k1);
+  if (!(i >= 1 && i <= gf.nx - 2 && j >= 1 && j <= gf.ny - 2) || k0 >= k1) return;
+  int I0, J0;
+  double tx, ty;
+  coarse_pos(i, gf.nx, gc.nx, map_mode(gf.nx, gc.nx), I0, tx);
+  coarse_pos(j, gf.ny, gc.ny, map_mode(gf.ny, gc.ny), J0, ty);
+  const int I1 = tx != 0.0 ? I0 + 1 : I0, J1 = ty != 0.0 ? J0 + 1 : J0;
+  const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
+  const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
+  // bilinear value on coarse plane K (boundary values through the closures)
+  auto bilinear = [&](int K) -> double {
+    double c00, c10, c01, c11;
+    if (!xy_edge && !(gf.dim == 3 && (K == 0 || K == gc.nz - 1))) {
+      const long long a = (long long)K * gc.sxy;
+      const long long r0 = (long long)J0 * gc.nx, r1 = (long long)J1 * gc.nx;
+      c00 = double(xc[a + r0 + I0]);
+      c10 = double(xc[a + r0 + I1]);
+      c01 = double(xc[a + r1 + I0]);
+      c11 = double(xc[a + r1 + I1]);
+    } else {
+      c00 = ext_value(gc, xc, I0, J0, K);
+      c10 = ext_value(gc, xc, I1, J0, K);
+      c01 = ext_value(gc, xc, I0, J1, K);
+      c11 = ext_value(gc, xc, I1, J1, K);
+    }
+    const double x0 = (1.0 - tx) * c00 + tx * c10, x1 = (1.0 - tx) * c01 + tx * c11;
+    return (1.0 - ty) * x0 + ty * x1;
+  };
+  int ka = -1, kb = -1;
+  double va = 0.0, vb = 0.0;
+  auto at = [&](int K) -> double {
+    if (K == ka) return va;
+    if (K == kb) return vb;
+    const double v = bilinear(K);
+    ka = kb;
+    va = vb;
+    kb = K;
+    vb = v;
+    return v;
+  };
+  for (int k = k0; k < k1; ++k) {
+    int K0 = 0;
+    double tz = 0.0;
+    if (gf.dim == 3) coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+    const double y0 = at(K0);
+    const double y1 = tz != 0.0 ? at(K0 + 1) : y0;
+    const double v = (1.0 - tz) * y0 + tz * y1;
+    const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
+    xf[id] = T(double(xf[id]) + v);
+  }
+}
+
 // Coarse k by injection from the nearest fine node (k_c(I) = k_f(2I) for odd n).
 __device__ __forceinline__ int nearest_fine(int I, int n, int nc) {
   return (I * (n - 1) + (nc - 1) / 2) / (nc - 1);

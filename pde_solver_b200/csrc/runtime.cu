@@ -120,6 +120,19 @@ dim3 stencil_grid_auto(const GridDev& g) {
   return dim3(xy.x, xy.y, cap_chunks(xyb, (int)chunks));
 }
 
+dim3 sweep_grid(const GridDev& g) {
+  const long long kTargetBlocks = 148 * 8;
+  const int kint = g.dim == 3 ? g.nz - 2 : 1;
+  const dim3 xy((g.nx + 31) / 32, (g.ny + 7) / 8, 1);
+  const long long xyb = (long long)xy.x * xy.y;
+  long long chunks = (kTargetBlocks + xyb - 1) / xyb;
+  // at least 16 planes per chunk so the two staging planes are amortised
+  const long long max_chunks = (kint + 15) / 16;
+  if (chunks > max_chunks) chunks = max_chunks;
+  if (chunks < 1) chunks = 1;
+  return dim3(xy.x, xy.y, cap_chunks(xyb, (int)chunks));
+}
+
 dim3 fused_grid(const GridDev& g) {
   const long long kTargetBlocks = 148 * 8;
   const int kint = g.dim == 3 ? g.nz - 2 : 1;

@@ -153,12 +153,10 @@ void Server::run_group(Context* ctx, std::vector<SReq*>& g) {
   }
   std::vector<pdeb200_report> reps(g.size());
   pdeb200_batch_solve(b, g.front()->tol, reps.data(), nullptr);
-  std::vector<double> packed((size_t)pdeb200_batch_nodes(b));
-  const pdeb200_status rs = pdeb200_batch_read(b, packed.data(), PDEB200_MEM_HOST);
   for (size_t q = 0; q < g.size(); ++q) {
     SReq* r = g[q];
-    const int64_t off = pdeb200_batch_offset(b, (int32_t)q);
-    if (rs == PDEB200_OK) std::memcpy(r->out, packed.data() + off, sizeof(double) * r->n);
+    // the result goes where the request's fields live (host or device)
+    const pdeb200_status rs = pdeb200_batch_read_member(b, (int32_t)q, r->out, r->prob.mem_space);
     r->res.status = rs != PDEB200_OK ? rs : (reps[q].converged ? PDEB200_OK : PDEB200_ERR_NOT_CONVERGED);
     r->res.iterations = reps[q].iterations;
     r->res.rel_residual = reps[q].rel_residual;
@@ -287,10 +285,13 @@ static void copy_problem(SReq* r, const pdeb200_problem* p) {
     dst->assign(src, src + cnt);
     return dst->data();
   };
-  r->prob.f = grab(p->f, n, &r->f);
-  r->prob.k = grab(p->k, n, &r->k);
-  r->prob.nodal = grab(p->nodal, 7 * n, &r->nodal);
-  r->prob.u0 = grab(p->u0, n, &r->u0);
+  // device-resident fields are used in place (the caller keeps them until the
+  // request completes); host fields are copied
+  const bool dev = p->mem_space == PDEB200_MEM_DEVICE;
+  r->prob.f = dev ? p->f : grab(p->f, n, &r->f);
+  r->prob.k = dev ? p->k : grab(p->k, n, &r->k);
+  r->prob.nodal = dev ? p->nodal : grab(p->nodal, 7 * n, &r->nodal);
+  r->prob.u0 = dev ? p->u0 : grab(p->u0, n, &r->u0);
   for (int f = 0; f < 6; ++f) {
     int w, h;
     face_dims_of(f, p->nx, p->ny, nz, &w, &h);

@@ -6,9 +6,11 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "host.h"
+#include "sweep.cuh"
 
 namespace pdeb {
 
@@ -359,6 +361,12 @@ inline bool coarse_dims(const GridDev& g, const pdeb200_problem* hp, int nc[3]) 
   return any;
 }
 
+// the z map of a level pair is the identity or nested 2:1 (host-side test of
+// z_marchable in kernels.cuh)
+inline bool z_nested(const GridDev& gf, const GridDev& gc) {
+  return gf.dim != 3 || gc.nz == gf.nz || 2 * gc.nz - 1 == gf.nz;
+}
+
 template <typename KT>
 inline void inject_k(Context* ctx, const GridDev& gf, const GridDev& gc, const KT* kf, KT* kc) {
   k_inject<KT><<<vec_blocks(gc.n, ctx), 256, 0, ctx->stream>>>(gf, gc, kf, kc);
@@ -431,7 +439,17 @@ struct Hierarchy {
     T* b;
     T* r;
     T* out;  // buffer holding this level's result after a V-cycle
+    bool single_pass = false;  // sweeps by k_rbgs_sweep (x_in -> x_out) instead of colour passes
   };
+  // With PDEB200_STAGED_SWEEP set, levels with at least this many nodes use
+  // the staged single-pass sweep (FP64 constant or divergence-form
+  // coefficients). It moves half the DRAM bytes of two colour passes but on
+  // B200 it is issue- and barrier-bound and about 10% slower at 257^3, so the
+  // colour passes stay the default.
+  static constexpr long long kSweepMinNodes = 1LL << 18;
+  static constexpr bool kSweepCoef =
+      std::is_same<T, double>::value &&
+      (std::is_same<Coef, CoefConst>::value || std::is_same<Coef, CoefDivk<double>>::value);
   std::vector<Level> levels;
   std::vector<Buf> owned;
   int pre = 2, post = 2, coarse_iters = 50;
@@ -516,9 +534,12 @@ struct Hierarchy {
     }
     // result buffer of each level after a V-cycle (fixed, so launches can be captured):
     // the first sweep from zero writes xa, every later sweep flips the buffer
+    const bool sweep_env = std::getenv("PDEB200_STAGED_SWEEP") != nullptr;
     for (size_t l = 0; l < levels.size(); ++l) {
       Level& L = levels[l];
-      if (!fused) {
+      L.single_pass = kSweepCoef && sweep_env && !fused && l + 1 < levels.size() && L.g.dim == 3 &&
+                      L.g.n >= kSweepMinNodes;
+      if (!fused && !L.single_pass) {
         L.out = L.xa;
         continue;
       }
@@ -540,6 +561,33 @@ struct Hierarchy {
                  const Ctl* ctl, int lvl) {
     const dim3 grid = stencil_grid_auto(L.g), block = stencil_block();
     const double dofs = interior_dofs(L.g);
+    if constexpr (kSweepCoef) {
+      if (L.single_pass) {
+        // per instantiation and device, before its first launch there
+        static bool attr_set[64] = {false};
+        const int dv = ctx->dev >= 0 && ctx->dev < 64 ? ctx->dev : 0;
+        if (!attr_set[dv]) {
+          PDEB_CUDA(cudaFuncSetAttribute(k_rbgs_sweep<Coef>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSwSmemBytes));
+          attr_set[dv] = true;
+        }
+        const dim3 sgrid = sweep_grid(L.g);
+        for (int s = 0; s < sweeps; ++s) {
+          const bool zero = from_zero && s == 0;
+          T* in = zero ? L.xb : cur;
+          T* out = zero ? L.xa : (cur == L.xa ? L.xb : L.xa);
+          {
+            // x read and written once, b and k read once: 32 B per DOF
+            ProfScope ps(ctx, "rbgs_sweep", lvl, dofs * 4.0 * sizeof(T));
+            k_rbgs_sweep<Coef><<<sgrid, kSwThreads, kSwSmemBytes, ctx->stream>>>(L.g, L.cf, b, in, out, first,
+                                                                                 zero ? 1 : 0, ctl);
+          }
+          ctx->count();
+          cur = out;
+        }
+        return cur;
+      }
+    }
     if (!fused) {
       // in place: the buffer never changes; flips are bookkeeping only
       if (from_zero) {
@@ -607,7 +655,11 @@ struct Hierarchy {
     Level& C = levels[l + 1];
     {
       ProfScope ps(ctx, "restrict", l, dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
-      k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+      if (z_nested(L.g, C.g))
+        k_restrict_march<T, T><<<stencil_grid_full(C.g, 8), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b,
+                                                                                                  ctl);
+      else
+        k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
     }
     if (needs_fold) {
       ProfScope ps(ctx, "restrict_fold", l, 0.0);
@@ -618,7 +670,10 @@ struct Hierarchy {
     level(ctx, l + 1, rhs0, ctl);
     {
       ProfScope ps(ctx, "prolong_add", l, dofs * sizeof(T) * (2.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
-      k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
+      if (z_nested(L.g, C.g))
+        k_prolong_march<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
+      else
+        k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
     }
     ctx->count();
     cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l);

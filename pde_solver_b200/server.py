@@ -45,20 +45,27 @@ class Server:
 
     def _submit(self, req, out, keep):
         rid = C.c_int64()
-        req.out = _dp(out)
+        # a device result buffer is passed as an int (device pointer)
+        req.out = C.cast(C.c_void_p(out), C.POINTER(C.c_double)) if isinstance(out, int) else _dp(out)
         st = self.lib.pdeb200_server_submit(self._h, C.byref(req), C.byref(rid))
         if st != abi.OK:
             raise ServerError(st, "submit refused")
         self._out[rid.value] = (out, keep)
         return rid.value
 
-    def submit_poisson(self, problem, tol=1e-10):
+    def submit_poisson(self, problem, tol=1e-10, out=None):
+        """Device-resident problems (mem_space MEM_DEVICE) need `out`, a device
+        pointer for the result; their arrays must outlive the request."""
         cp = problem.to_c()
         req = abi.Request()
         req.kind = abi.REQ_POISSON
         req.problem = C.pointer(cp)
         req.tol = tol
-        return self._submit(req, np.empty(problem.n), (problem, cp))
+        if problem.mem_space == abi.MEM_DEVICE:
+            if out is None:
+                raise ValueError("device-resident requests need a device result pointer")
+            return self._submit(req, int(out), (problem, cp))
+        return self._submit(req, np.empty(problem.n) if out is None else out, (problem, cp))
 
     def submit_heat(self, problem, dt, steps, t_start=0.0):
         cp = problem.to_c()

@@ -220,3 +220,23 @@ def test_graph_replay_matches_direct_launches(monkeypatch):
     assert ra.iterations == rb.iterations
     assert np.array_equal(a, b)
     assert ra.kernel_launches == rb.kernel_launches
+
+
+@pytest.mark.parametrize("which", ["divk", "const"])
+def test_staged_sweep_matches_colour_passes(monkeypatch, which):
+    # with PDEB200_STAGED_SWEEP, levels of 2^18+ nodes smooth with the
+    # single-pass staged sweep; it does the arithmetic of two colour passes,
+    # so fields agree to rounding
+    if which == "divk":
+        p = synthetic.varcoef_poisson_3d(65, seed=21)
+    else:
+        p = GridProblem(65, 70, 66, a=-1.0, b=-1.0, az=-1.0)
+        p.f = np.random.Generator(np.random.PCG64(2)).standard_normal(p.n)
+        p.faces = [FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(1.0),
+                   FaceBC.neumann(0.1), FaceBC.dirichlet(0.0)]
+    opt = default_options(method=abi.MG_PCG, tol=1e-11, tol_mode=abi.TOL_RELATIVE, max_iter=200)
+    a, ra = solver.solve(p, opt)
+    monkeypatch.setenv("PDEB200_STAGED_SWEEP", "1")
+    b, rb = solver.solve(p, opt)
+    assert abs(ra.iterations - rb.iterations) <= 1
+    assert rel_l2(a, b) <= 1e-10

@@ -114,3 +114,32 @@ def test_fp64_lanes_match_single_call():
         assert res.status == abi.OK and res.group_size == 1
         ref, _ = solver.solve(p, opt)
         assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("precision", [abi.MIXED, abi.FP64])
+def test_device_resident_requests_match_host_requests(precision):
+    # k and f already in HBM are used in place, and the result is written to
+    # a device buffer; the numbers are those of the same request from host data
+    import copy
+
+    import torch
+
+    ps = poisson_mix()[:4]
+    dev = torch.device("cuda", 0)
+    keep, dps, outs = [], [], []
+    for p in ps:
+        q = copy.copy(p)
+        k = torch.from_numpy(p.k).to(dev)
+        f = torch.from_numpy(p.f).to(dev)
+        keep += [k, f]
+        q.k, q.f, q.mem_space, q.k_dev, q.f_dev = None, None, abi.MEM_DEVICE, k.data_ptr(), f.data_ptr()
+        dps.append(q)
+        outs.append(torch.empty(p.n, dtype=torch.float64, device=dev))
+    torch.cuda.synchronize()
+    with Server(lanes=2, precision=precision) as s:
+        host = [s.wait(s.submit_poisson(p))[0] for p in ps]
+        ids = [s.submit_poisson(q, out=o.data_ptr()) for q, o in zip(dps, outs)]
+        res = [s.wait(i)[1] for i in ids]
+    assert all(r.status == abi.OK for r in res)
+    for h, o in zip(host, outs):
+        assert np.array_equal(h, o.cpu().numpy())
