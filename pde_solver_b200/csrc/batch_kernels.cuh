@@ -418,10 +418,31 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
   const BLevel& L = lv[T.lev];
   const KT* k = static_cast<const KT*>(L.kh);
   float* __restrict__ x = L.x;
+  // In one colour pass no node is both written and read (updated nodes read
+  // only the other colour), so the reads go through a separate read-only
+  // view and the loads of later nodes can overlap earlier stores.
+  const float* __restrict__ xr = L.x;
   const float* __restrict__ b = L.b;
   const int nx = L.g.nx, dim = L.g.dim;
   const long long sxy = L.g.sxy;
   const bool is3 = dim == 3;
+  if (!is3 && !from_zero) {
+    // 2D: threads walk only the cells of the colour being updated
+    const int half = (int(T.w) + 1) >> 1;
+    const int total = int(T.h) * half;
+    const int i0 = 1 + T.x0;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int row = t / half, c = t - row * half;
+      const int j = 1 + T.y0 + row;
+      const int ra = 2 * c + ((i0 + j + color) & 1);
+      if (ra >= int(T.w)) continue;
+      const int i = i0 + ra;
+      const long long id = (long long)j * nx + i;
+      const Stencil<float> s = bstencil<float, KT>(L, k, i, j, 0, id, nullptr);
+      x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], 0.f, 0.f, dim)) / s.c;
+    }
+    return;
+  }
   tile_columns(T, [&](int i, int j) {
     if (from_zero) {
       for (int kk = T.z0; kk < T.z1; ++kk) {
@@ -434,12 +455,13 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
         }
       }
     } else {
+#pragma unroll 2
       for (int kk = T.z0 + ((i + j + T.z0 + color) & 1); kk < T.z1; kk += 2) {
         const long long id = bid(L.g, i, j, kk);
         const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
-        const float zp = is3 ? x[id + sxy] : 0.f;
-        const float zm = is3 ? x[id - sxy] : 0.f;
-        x[id] = (b[id] - nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, dim)) / s.c;
+        const float zp = is3 ? xr[id + sxy] : 0.f;
+        const float zm = is3 ? xr[id - sxy] : 0.f;
+        x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], zp, zm, dim)) / s.c;
       }
     }
   });

@@ -74,6 +74,30 @@ struct CoefDivk {
   double cx, dyc, dzc, e;   // c/(2dx), d/(2dy), dz/(2dz), e
   template <typename T>
   __device__ __forceinline__ Stencil<T> at(const GridDev& g, long long id) const {
+    if constexpr (sizeof(T) == 4) {
+      // FP32 stencils (preconditioner levels of the precision form) in FP32
+      const float kc = float(load_k(k, id));
+      const float kxm = 0.5f * (kc + float(load_k(k, id - 1))), kxp = 0.5f * (kc + float(load_k(k, id + 1)));
+      const float kym = 0.5f * (kc + float(load_k(k, id - g.nx))), kyp = 0.5f * (kc + float(load_k(k, id + g.nx)));
+      const float fx = float(ihx2), fy = float(ihy2);
+      Stencil<T> s;
+      s.xm = T(-kxm * fx - float(cx));
+      s.xp = T(-kxp * fx + float(cx));
+      s.ym = T(-kym * fy - float(dyc));
+      s.yp = T(-kyp * fy + float(dyc));
+      float c = (kxm + kxp) * fx + (kym + kyp) * fy;
+      if (g.dim == 3) {
+        const float fz = float(ihz2);
+        const float kzm = 0.5f * (kc + float(load_k(k, id - g.sxy))), kzp = 0.5f * (kc + float(load_k(k, id + g.sxy)));
+        s.zm = T(-kzm * fz - float(dzc));
+        s.zp = T(-kzp * fz + float(dzc));
+        c += (kzm + kzp) * fz;
+      } else {
+        s.zm = s.zp = T(0);
+      }
+      s.c = T(c + float(e));
+      return s;
+    }
     const double kc = load_k(k, id);
     const double kxm = 0.5 * (kc + load_k(k, id - 1)), kxp = 0.5 * (kc + load_k(k, id + 1));
     const double kym = 0.5 * (kc + load_k(k, id - g.nx)), kyp = 0.5 * (kc + load_k(k, id + g.nx));
