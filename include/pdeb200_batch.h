@@ -18,7 +18,8 @@
  * Tile shapes and smoother schedule come from pdeb200_batch_options or from
  * the autotuner, which times candidate schedules on the batch itself and
  * keeps the winner in an on-disk cache keyed by the device and the batch's
- * shapes. */
+ * shapes. As members converge, the tile tables are rebuilt for the
+ * unfinished ones (compaction), which changes no member's numbers. */
 #ifndef PDEB200_BATCH_H
 #define PDEB200_BATCH_H
 
@@ -46,7 +47,8 @@ typedef struct {
   double inner_tol;        /* inner relative tolerance; 0 = 1e-4 */
   const char* tune_cache;  /* autotuner cache file; NULL = $PDEB200_TUNE_CACHE, else none */
   void* stream;            /* cudaStream_t for all work; NULL = the batch's own stream */
-  int32_t reserved[8];
+  int32_t no_compact;      /* 1: keep every member's tiles in the launches until the solve ends */
+  int32_t reserved[7];
 } pdeb200_batch_options;
 
 typedef struct {
@@ -62,7 +64,8 @@ typedef struct {
   double tune_ms;          /* autotuning time at create (0 when cached or off) */
   int32_t tuned_from_cache;
   int32_t graph;           /* 1 when the cycle ran as a CUDA graph */
-  int32_t reserved[6];
+  int32_t compactions;     /* times the tables were rebuilt for the unfinished members */
+  int32_t reserved[5];
 } pdeb200_batch_stats;
 
 void pdeb200_batch_default_options(pdeb200_batch_options* opt);

@@ -177,7 +177,8 @@ class BatchOptions(C.Structure):
         ("inner_tol", C.c_double),
         ("tune_cache", C.c_char_p),
         ("stream", C.c_void_p),
-        ("reserved", C.c_int32 * 8),
+        ("no_compact", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -196,7 +197,8 @@ class BatchStats(C.Structure):
         ("tune_ms", C.c_double),
         ("tuned_from_cache", C.c_int32),
         ("graph", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("compactions", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -26,6 +27,8 @@ struct BatchParams {
   int max_inner = 40, max_outer = 12;
   double inner_tol = 1e-4;
 };
+
+struct Sched;
 
 struct BatchPlan {
   int dev = 0;
@@ -47,23 +50,46 @@ struct BatchPlan {
   Buf a64, a32, akh;               // packed arenas
   double *f64 = nullptr, *b64 = nullptr, *x64 = nullptr;
   std::vector<Buf> owned;          // face arrays of coarse levels
-  Buf d_levels, d_mem, d_tiles, d_partials, d_active;
-  std::vector<long long> tile_off, tile_cnt;
+  Buf d_levels, d_mem, d_active;
+  std::unique_ptr<Sched> full;  // tiles of every member (set by build_schedule)
   int* h_active = nullptr;
   BMember* h_mem = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  long long launches_per_cycle = 0;
+  bool compact = true;  // rebuild the tables for the unfinished members as they thin out
+  int last_compactions = 0;
   long long last_launches = 0;
   int last_cycles = 0;
   double last_ms = 0.0, tune_ms = 0.0;
   bool tuned_from_cache = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-  ~BatchPlan() {
-    if (stream) cudaStreamSynchronize(stream);
-    if (gexec) cudaGraphExecDestroy(gexec);
+  ~BatchPlan();
+};
+
+// Tile tables of one schedule (all members, or the unfinished ones), the
+// reduction partials sized for its level-0 tiles, each member's level-0 tile
+// range and the captured cycle.
+struct Sched {
+  Buf tiles, partials;
+  std::vector<long long> off, cnt;
+  std::vector<int> tile0, ntiles;  // per member; ntiles 0 when absent
+  int lmax = 0;
+  int members = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;
+  Sched() = default;
+  Sched(const Sched&) = delete;
+  Sched& operator=(const Sched&) = delete;
+  ~Sched() {
+    if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+BatchPlan::~BatchPlan() {
+  {
+    if (stream) cudaStreamSynchronize(stream);
+    full.reset();
     if (h_active) cudaFreeHost(h_active);
     if (h_mem) cudaFreeHost(h_mem);
     if (ev0) cudaEventDestroy(ev0);
@@ -75,13 +101,11 @@ struct BatchPlan {
     akh.reset();
     d_levels.reset();
     d_mem.reset();
-    d_tiles.reset();
-    d_partials.reset();
     d_active.reset();
     if (stream) cudaStreamSynchronize(stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
-};
+}
 
 namespace {
 
@@ -131,23 +155,23 @@ void make_tiles(const GridDev& g, bool coarse, const BatchParams& p, int lev, in
 }
 
 template <typename KT>
-void enqueue_cycle(BatchPlan& B) {
-  const BTile* tiles = B.d_tiles.as<BTile>();
+void enqueue_cycle(BatchPlan& B, Sched& Sc) {
+  const BTile* tiles = Sc.tiles.as<BTile>();
   const BLevel* lv = B.d_levels.as<BLevel>();
   BMember* mem = B.d_mem.as<BMember>();
-  double* part = B.d_partials.as<double>();
+  double* part = Sc.partials.as<double>();
   int* active = B.d_active.as<int>();
   cudaStream_t s = B.stream;
   const int T = kBThreads;
-  auto S = [&](int l) { return tiles + B.tile_off[l]; };
-  auto N = [&](int l) { return (unsigned)B.tile_cnt[l]; };
+  auto S = [&](int l) { return tiles + Sc.off[l]; };
+  auto N = [&](int l) { return (unsigned)Sc.cnt[l]; };
   long long launches = 0;
   kb_xupdate<<<N(0), T, 0, s>>>(S(0), lv, mem);
   kb_outer<<<N(0), T, 0, s>>>(S(0), lv, mem, part, active);
   kb_apply_pq<<<N(0), T, 0, s>>>(S(0), lv, mem, part);
   kb_update<<<N(0), T, 0, s>>>(S(0), lv, mem, part);
   launches += 4;
-  for (int l = 0; l + 1 < B.lmax; ++l) {
+  for (int l = 0; l + 1 < Sc.lmax; ++l) {
     for (int q = 0; q < B.prm.pre; ++q) {
       kb_smooth<KT><<<N(l), T, 0, s>>>(S(l), lv, mem, 0, q == 0 ? 1 : 0);
       kb_smooth<KT><<<N(l), T, 0, s>>>(S(l), lv, mem, 1, 0);
@@ -157,7 +181,7 @@ void enqueue_cycle(BatchPlan& B) {
     kb_restrict<KT><<<N(l + 1), T, 0, s>>>(S(l + 1), lv, mem, B.prm.coarse_sweeps);
     launches += 2;
   }
-  for (int l = B.lmax - 2; l >= 0; --l) {
+  for (int l = Sc.lmax - 2; l >= 0; --l) {
     kb_prolong<<<N(l), T, 0, s>>>(S(l), lv, mem);
     ++launches;
     for (int q = 0; q < B.prm.post; ++q) {
@@ -169,68 +193,77 @@ void enqueue_cycle(BatchPlan& B) {
   kb_rz<<<N(0), T, 0, s>>>(S(0), lv, mem, part);
   kb_pupdate<<<N(0), T, 0, s>>>(S(0), lv, mem);
   launches += 2;
-  B.launches_per_cycle = launches;
+  Sc.launches = launches;
   PDEB_CUDA(cudaGetLastError());
 }
 
-void run_cycle_enqueue(BatchPlan& B) {
+void run_cycle_enqueue(BatchPlan& B, Sched& Sc) {
   if (B.bf16)
-    enqueue_cycle<__nv_bfloat16>(B);
+    enqueue_cycle<__nv_bfloat16>(B, Sc);
   else
-    enqueue_cycle<float>(B);
+    enqueue_cycle<float>(B, Sc);
 }
 
-// Tile tables, member tile ranges and the captured cycle for the current
-// parameters.
-void build_schedule(BatchPlan& B) {
-  if (B.gexec) {
-    cudaGraphExecDestroy(B.gexec);
-    B.gexec = nullptr;
+// Tile tables of `subset` (every member when null), member tile ranges and the
+// captured cycle for the current parameters.
+std::unique_ptr<Sched> make_sched(BatchPlan& B, const std::vector<int>* subset) {
+  auto Sc = std::make_unique<Sched>();
+  std::vector<int> all_m;
+  if (!subset) {
+    all_m.resize(B.count);
+    for (int m = 0; m < B.count; ++m) all_m[m] = m;
+    subset = &all_m;
   }
-  if (B.graph) {
-    cudaGraphDestroy(B.graph);
-    B.graph = nullptr;
-  }
-  std::vector<std::vector<BTile>> per(B.lmax);
-  for (int m = 0; m < B.count; ++m) {
+  Sc->members = (int)subset->size();
+  for (int m : *subset) Sc->lmax = std::max(Sc->lmax, B.nlev[m]);
+  Sc->tile0.assign(B.count, 0);
+  Sc->ntiles.assign(B.count, 0);
+  std::vector<std::vector<BTile>> per(Sc->lmax);
+  for (int m : *subset) {
     for (int l = 0; l < B.nlev[m]; ++l) {
       const int rec = B.lev0[m] + l;
       const BLevel& L = B.levels[rec];
-      if (l == 0) {
-        B.mem_tmpl[m].tile0 = (int)per[0].size();
-      }
+      if (l == 0) Sc->tile0[m] = (int)per[0].size();
       make_tiles(L.g, L.coarsest != 0, B.prm, rec, m, &per[l]);
-      if (l == 0) B.mem_tmpl[m].ntiles = (int)per[0].size() - B.mem_tmpl[m].tile0;
+      if (l == 0) Sc->ntiles[m] = (int)per[0].size() - Sc->tile0[m];
     }
   }
   std::vector<BTile> all;
-  B.tile_off.assign(B.lmax, 0);
-  B.tile_cnt.assign(B.lmax, 0);
-  for (int l = 0; l < B.lmax; ++l) {
-    B.tile_off[l] = (long long)all.size();
-    B.tile_cnt[l] = (long long)per[l].size();
+  Sc->off.assign(Sc->lmax, 0);
+  Sc->cnt.assign(Sc->lmax, 0);
+  for (int l = 0; l < Sc->lmax; ++l) {
+    Sc->off[l] = (long long)all.size();
+    Sc->cnt[l] = (long long)per[l].size();
     all.insert(all.end(), per[l].begin(), per[l].end());
   }
-  if (B.tile_cnt[0] >= (1LL << 31)) throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "batch has too many tiles"};
-  B.d_tiles = Buf(sizeof(BTile) * all.size(), B.stream);
-  PDEB_CUDA(cudaMemcpyAsync(B.d_tiles.as<void>(), all.data(), sizeof(BTile) * all.size(), cudaMemcpyHostToDevice,
+  if (Sc->cnt[0] >= (1LL << 31)) throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "batch has too many tiles"};
+  Sc->tiles = Buf(sizeof(BTile) * all.size(), B.stream);
+  PDEB_CUDA(cudaMemcpyAsync(Sc->tiles.as<void>(), all.data(), sizeof(BTile) * all.size(), cudaMemcpyHostToDevice,
                             B.stream));
-  B.d_partials = Buf(sizeof(double) * (size_t)B.tile_cnt[0], B.stream);
+  Sc->partials = Buf(sizeof(double) * (size_t)Sc->cnt[0], B.stream);
   PDEB_CUDA(cudaStreamSynchronize(B.stream));
   if (B.use_graph) {
     PDEB_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
     try {
-      run_cycle_enqueue(B);
+      run_cycle_enqueue(B, *Sc);
     } catch (...) {
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(B.stream, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
-    PDEB_CUDA(cudaStreamEndCapture(B.stream, &B.graph));
-    PDEB_CUDA(cudaGraphInstantiate(&B.gexec, B.graph, 0));
-  } else {
-    B.launches_per_cycle = 0;
+    PDEB_CUDA(cudaStreamEndCapture(B.stream, &Sc->graph));
+    PDEB_CUDA(cudaGraphInstantiate(&Sc->exec, Sc->graph, 0));
+  }
+  return Sc;
+}
+
+void build_schedule(BatchPlan& B) {
+  B.full.reset();
+  B.full = make_sched(B, nullptr);
+  for (int m = 0; m < B.count; ++m) {
+    B.mem_tmpl[m].tile0 = B.full->tile0[m];
+    B.mem_tmpl[m].ntiles = B.full->ntiles[m];
   }
 }
 
@@ -257,29 +290,56 @@ int solve_all(BatchPlan& B, double tol, int max_cycles_cap = 0) {
   PDEB_CUDA(cudaMemcpyAsync(B.d_mem.as<void>(), B.h_mem, sizeof(BMember) * B.count, cudaMemcpyHostToDevice,
                             B.stream));
   PDEB_CUDA(cudaMemcpyAsync(B.d_active.as<void>(), B.h_active, sizeof(int), cudaMemcpyHostToDevice, B.stream));
-  const BTile* tiles = B.d_tiles.as<BTile>();
   const BLevel* lv = B.d_levels.as<BLevel>();
-  kb_rhs<<<(unsigned)B.tile_cnt[0], kBThreads, 0, B.stream>>>(tiles, lv, B.d_mem.as<BMember>());
+  kb_rhs<<<(unsigned)B.full->cnt[0], kBThreads, 0, B.stream>>>(B.full->tiles.as<BTile>(), lv,
+                                                               B.d_mem.as<BMember>());
   long long launches = 1;
   const int max_cycles =
       max_cycles_cap > 0 ? max_cycles_cap : B.prm.max_outer * (B.prm.max_inner + 2) + 8;
-  int cycles = 0, batch = 2;
+  Sched* cur = B.full.get();
+  std::unique_ptr<Sched> part;  // tables of the unfinished members, once they thin out
+  int compactions = 0;
+  int cycles = 0, batch = 2, prev_active = B.count;
   while (cycles < max_cycles) {
     const int nb = std::min(batch, max_cycles - cycles);
     for (int q = 0; q < nb; ++q) {
-      if (B.gexec) {
-        PDEB_CUDA(cudaGraphLaunch(B.gexec, B.stream));
+      if (cur->exec) {
+        PDEB_CUDA(cudaGraphLaunch(cur->exec, B.stream));
       } else {
-        run_cycle_enqueue(B);
+        run_cycle_enqueue(B, *cur);
       }
-      launches += B.launches_per_cycle;
+      launches += cur->launches;
     }
     cycles += nb;
     PDEB_CUDA(cudaMemcpyAsync(B.h_active, B.d_active.as<void>(), sizeof(int), cudaMemcpyDeviceToHost, B.stream));
     PDEB_CUDA(cudaStreamSynchronize(B.stream));
     if (*B.h_active <= 0) break;
-    batch = std::min(batch * 2, 8);
+    // poll often once members finish (compaction follows them), rarely before
+    batch = *B.h_active < prev_active ? 2 : std::min(batch * 2, 8);
+    prev_active = *B.h_active;
+    // Compaction: when at most half the members in the tables are unfinished,
+    // rebuild the tables (and the captured cycle) for those alone. A member's
+    // tiles and their order do not change, so neither do its numbers.
+    if (B.compact && *B.h_active * 2 <= cur->members && compactions < 4) {
+      PDEB_CUDA(cudaMemcpyAsync(B.h_mem, B.d_mem.as<void>(), sizeof(BMember) * B.count, cudaMemcpyDeviceToHost,
+                                B.stream));
+      PDEB_CUDA(cudaStreamSynchronize(B.stream));
+      std::vector<int> act;
+      for (int m = 0; m < B.count; ++m)
+        if (B.h_mem[m].state != kBDone) act.push_back(m);
+      std::unique_ptr<Sched> next = make_sched(B, &act);
+      for (int m : act) {
+        B.h_mem[m].tile0 = next->tile0[m];
+        B.h_mem[m].ntiles = next->ntiles[m];
+      }
+      PDEB_CUDA(cudaMemcpyAsync(B.d_mem.as<void>(), B.h_mem, sizeof(BMember) * B.count, cudaMemcpyHostToDevice,
+                                B.stream));
+      part = std::move(next);
+      cur = part.get();
+      ++compactions;
+    }
   }
+  B.last_compactions = compactions;
   kb_fill_boundary<<<B.count, kBThreads, 0, B.stream>>>(lv, B.d_mem.as<BMember>());
   ++launches;
   PDEB_CUDA(cudaGetLastError());
@@ -352,6 +412,7 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
   B.count = count;
   B.bf16 = o->bf16_coefficients != 0;
   B.use_graph = o->no_graph == 0;
+  B.compact = o->no_compact == 0;
   B.dev = o->device;
   get_context(o->device);
   if (o->stream) {
@@ -804,10 +865,10 @@ pdeb200_status pdeb200_batch_solve(pdeb200_batch* b, double tol, pdeb200_report*
     stats->cycles = B.last_cycles;
     stats->max_levels = B.lmax;
     stats->kernel_launches = B.last_launches;
-    stats->tiles_level0 = B.tile_cnt.empty() ? 0 : B.tile_cnt[0];
+    stats->tiles_level0 = B.full ? B.full->cnt[0] : 0;
     stats->nodes = B.nodes;
     size_t bytes = B.a64.bytes() + B.a32.bytes() + B.akh.bytes() + B.d_levels.bytes() + B.d_mem.bytes() +
-                   B.d_tiles.bytes() + B.d_partials.bytes();
+                   (B.full ? B.full->tiles.bytes() + B.full->partials.bytes() : 0);
     for (const auto& P : B.probs)
       for (const auto& buf : P.owned) bytes += buf.bytes();
     for (const auto& buf : B.owned) bytes += buf.bytes();
@@ -815,7 +876,8 @@ pdeb200_status pdeb200_batch_solve(pdeb200_batch* b, double tol, pdeb200_report*
     stats->device_ms = B.last_ms;
     stats->tune_ms = B.tune_ms;
     stats->tuned_from_cache = B.tuned_from_cache ? 1 : 0;
-    stats->graph = B.gexec ? 1 : 0;
+    stats->graph = B.full && B.full->exec ? 1 : 0;
+    stats->compactions = B.last_compactions;
   }
   return first_bad;
 }
@@ -864,6 +926,7 @@ pdeb200_status pdeb200_batch_get_options(const pdeb200_batch* b, pdeb200_batch_o
   o->max_outer = B.prm.max_outer;
   o->bf16_coefficients = B.bf16 ? 1 : 0;
   o->no_graph = B.use_graph ? 0 : 1;
+  o->no_compact = B.compact ? 0 : 1;
   o->inner_tol = B.prm.inner_tol;
   o->stream = B.own_stream ? nullptr : B.stream;
   return PDEB200_OK;

@@ -176,3 +176,27 @@ def test_batch_rejects_unsupported_members():
     with pytest.raises(BatchError) as e:
         Batch([q])
     assert e.value.status == abi.ERR_UNSUPPORTED
+
+
+def test_compaction_changes_no_numbers(batch_result, members):
+    # rebuilding the tables for the unfinished members keeps every member's
+    # tiles and their order, so the fields are the same bits
+    _, fields, stats = batch_result
+    with Batch(members, no_compact=1, **FIXED) as b:
+        b.solve(TOL)
+        assert b.stats.compactions == 0
+        got = b.read()
+    for u, v in zip(got, fields):
+        assert np.array_equal(u, v)
+    ms = synthetic.batch_members(40, 8, seed=3, hi2=257, hi3=49)
+    for p in ms[::2]:
+        p.f = np.zeros(p.n)  # these finish at the first outer step
+    with Batch(ms, **FIXED) as b:
+        b.solve(TOL)
+        compacted = b.read()
+        assert b.stats.compactions >= 1
+    with Batch(ms, no_compact=1, **FIXED) as b:
+        b.solve(TOL)
+        plain = b.read()
+    for u, v in zip(compacted, plain):
+        assert np.array_equal(u, v)
