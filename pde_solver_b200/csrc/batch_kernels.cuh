@@ -568,7 +568,59 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
   float* __restrict__ bc = C.b;
   const bool zmarch = gc.dim != 3 || map_mode(F.g.nz, gc.nz) <= 1;
   const bool zsame = gc.dim == 3 && gc.nz == F.g.nz;
+  const int xm = map_mode(F.g.nx, gc.nx), ym = map_mode(F.g.ny, gc.ny);
+  // nested 2:1 or identity in every dimension: FP32 weights {1/4, 1/2, 1/4}
+  // (or {0, 1, 0}) on the three fine nodes around each interior coarse node,
+  // always inside the fine grid, no clipping
+  const bool fast = xm <= 1 && ym <= 1 && zmarch;
+  const int fnx = F.g.nx;
+  const long long fsxy = F.g.sxy;
   tile_columns(T, [&](int I, int J) {
+    if (fast) {
+      const int fi = (xm == 1 ? 2 * I : I) - 1, fj = (ym == 1 ? 2 * J : J) - 1;
+      const float wx0 = xm == 1 ? 0.25f : 0.f, wx1 = xm == 1 ? 0.5f : 1.f;
+      const float wy0 = ym == 1 ? 0.25f : 0.f, wy1 = ym == 1 ? 0.5f : 1.f;
+      auto plane = [&](int fk) -> float {
+        const float* r0 = rf + (long long)fk * fsxy + (long long)fj * fnx + fi;
+        const float s0 = wx0 * r0[0] + wx1 * r0[1] + wx0 * r0[2];
+        const float* r1 = r0 + fnx;
+        const float s1 = wx0 * r1[0] + wx1 * r1[1] + wx0 * r1[2];
+        const float* r2 = r1 + fnx;
+        const float s2 = wx0 * r2[0] + wx1 * r2[1] + wx0 * r2[2];
+        return wy0 * s0 + wy1 * s1 + wy0 * s2;
+      };
+      const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
+      const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
+      float below = gc.dim == 3 && !zsame ? plane(2 * T.z0 - 1) : 0.f;
+      for (int K = T.z0; K < T.z1; ++K) {
+        float acc;
+        if (gc.dim != 3) {
+          acc = plane(0);
+        } else if (zsame) {
+          acc = plane(K);
+        } else {
+          const float mid = plane(2 * K), above = plane(2 * K + 1);
+          acc = 0.25f * below + 0.5f * mid + 0.25f * above;
+          below = above;
+        }
+        const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+        if (dxl | dxh | dyl | dyh | dzl | dzh) {
+          double fold = 0.0;
+          for (int dk = dzl; dk <= dzh; ++dk)
+            for (int dj = dyl; dj <= dyh; ++dj)
+              for (int di = dxl; di <= dxh; ++di) {
+                if (di == 0 && dj == 0 && dk == 0) continue;
+                int ci = I + di, cj = J + dj, ck = K + dk;
+                const double coef = ext_chain(gc, ci, cj, ck);
+                if (coef != 0.0 && ci == I && cj == J && ck == K)
+                  fold += coef * full_weight<float>(F.g, gc, rf, I + di, J + dj, K + dk);
+              }
+          acc = float(double(acc) + fold);
+        }
+        bc[bid(gc, I, J, K)] = acc;
+      }
+      return;
+    }
     const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
     const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
     FwColumn<float> col;
@@ -624,6 +676,53 @@ __global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict_
   float* __restrict__ xf = F.x;
   const int xmode = map_mode(gf.nx, gc.nx), ymode = map_mode(gf.ny, gc.ny);
   const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
+  if (xmode <= 1 && ymode <= 1 && zmode <= 1) {
+    // nested 2:1 or identity in every dimension: interpolation weights are 1
+    // or 1/2, in FP32, loading only the coarse values a node uses
+    tile_columns(T, [&](int i, int j) {
+      const bool ax = xmode == 1 && (i & 1), ay = ymode == 1 && (j & 1);
+      const int I0 = xmode == 1 ? i >> 1 : i, J0 = ymode == 1 ? j >> 1 : j;
+      const int I1 = ax ? I0 + 1 : I0, J1 = ay ? J0 + 1 : J0;
+      const bool xy_edge = I0 == 0 || I1 == gc.nx - 1 || J0 == 0 || J1 == gc.ny - 1;
+      auto bil = [&](int K) -> float {
+        const bool edge = xy_edge || (gf.dim == 3 && (K == 0 || K == gc.nz - 1));
+        auto cv = [&](int I, int J) -> float {
+          return edge ? float(ext_value(gc, xc, I, J, K)) : xc[(long long)K * gc.sxy + (long long)J * gc.nx + I];
+        };
+        const float c00 = cv(I0, J0);
+        if (!ax && !ay) return c00;
+        if (!ay) return 0.5f * (c00 + cv(I1, J0));
+        if (!ax) return 0.5f * (c00 + cv(I0, J1));
+        return 0.25f * ((c00 + cv(I1, J0)) + (cv(I0, J1) + cv(I1, J1)));
+      };
+      if (gf.dim != 3) {
+        const long long id = bid(gf, i, j, 0);
+        xf[id] += bil(0);
+        return;
+      }
+      // march in z: each coarse plane's value is computed once and shared by
+      // the fine planes it feeds
+      int ka = -1, kb = -1;
+      float va = 0.f, vb = 0.f;
+      auto at = [&](int K) -> float {
+        if (K == kb) return vb;
+        if (K == ka) return va;
+        ka = kb;
+        va = vb;
+        kb = K;
+        vb = bil(K);
+        return vb;
+      };
+      for (int k = T.z0; k < T.z1; ++k) {
+        const int K0 = zmode == 1 ? k >> 1 : k;
+        const bool az = zmode == 1 && (k & 1);
+        const float v = az ? 0.5f * (at(K0) + at(K0 + 1)) : at(K0);
+        const long long id = bid(gf, i, j, k);
+        xf[id] += v;
+      }
+    });
+    return;
+  }
   tile_columns(T, [&](int i, int j) {
     int I0, J0;
     double tx, ty;

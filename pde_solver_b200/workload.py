@@ -24,13 +24,25 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="varcoef3d", choices=["varcoef3d", "convdiff3d"])
     ap.add_argument("--batch", default="", help="n2d,n3d: batched workload instead of one grid")
     ap.add_argument("--bf16", action="store_true")
+    ap.add_argument("--tuned", action="store_true", help="batch schedule from pde_solver_b200/batch_tune_cache.txt")
+    ap.add_argument("--retune", default="", help="autotune the batch and append the result to this cache file")
     a = ap.parse_args(argv)
     if a.batch:
         from .batch import Batch
 
         n2d, n3d = (int(v) for v in a.batch.split(","))
         ms = synthetic.batch_members(n2d, n3d)
-        b = Batch(ms, bf16_coefficients=1 if a.bf16 else 0)
+        import os
+
+        kw = {}
+        if a.retune:
+            kw = dict(autotune=1, tune_cache=a.retune)
+        elif a.tuned:
+            kw = dict(autotune=1, tune_cache=os.path.join(os.path.dirname(__file__), "batch_tune_cache.txt"))
+        b = Batch(ms, bf16_coefficients=1 if a.bf16 else 0, **kw)
+        o = b.options()
+        print(f"schedule tile=({o.tile_x},{o.tile_y},{o.tile_z}) pre={o.pre_smooth} post={o.post_smooth} "
+              f"inner_tol={o.inner_tol:g}", flush=True)
         for _ in range(a.solves):
             b.solve(1e-10)
             s = b.stats
