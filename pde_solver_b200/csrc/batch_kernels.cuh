@@ -126,6 +126,82 @@ __device__ __forceinline__ Stencil<T> bstencil(const BLevel& L, const KT* k, int
   return s;
 }
 
+// FP32 folded stencil of one level with its scalars in registers, loaded once
+// per block (the level descriptor stays in global memory for the face data,
+// read only at face-adjacent nodes). Indices are 32-bit offsets within the
+// level's arrays (a member level has fewer than 2^31 nodes).
+template <typename KT>
+struct FStencil {
+  int nx, ny, nz, dim, sxy, kind;
+  float ihx2, ihy2, ihz2, cx, dyc, dzc, e;
+  float c0, xm0, xp0, ym0, yp0, zm0, zp0;
+  const KT* k;
+  const GridDev* g;
+  __device__ __forceinline__ void load(const BLevel& L, const KT* kk) {
+    nx = L.g.nx;
+    ny = L.g.ny;
+    nz = L.g.nz;
+    dim = L.g.dim;
+    sxy = int(L.g.sxy);
+    kind = L.kind;
+    ihx2 = float(L.ihx2);
+    ihy2 = float(L.ihy2);
+    ihz2 = float(L.ihz2);
+    cx = float(L.cx);
+    dyc = float(L.dyc);
+    dzc = float(L.dzc);
+    e = float(L.e);
+    c0 = float(L.cc.c);
+    xm0 = float(L.cc.xm);
+    xp0 = float(L.cc.xp);
+    ym0 = float(L.cc.ym);
+    yp0 = float(L.cc.yp);
+    zm0 = float(L.cc.zm);
+    zp0 = float(L.cc.zp);
+    k = kk;
+    g = &L.g;
+  }
+  __device__ __forceinline__ float kv(int id) const {
+    if constexpr (sizeof(KT) == 2)
+      return __bfloat162float(k[id]);
+    else
+      return __ldg(k + id);
+  }
+  __device__ __forceinline__ Stencil<float> at(int i, int j, int kz, int id) const {
+    Stencil<float> s;
+    if (kind == kConst) {
+      s.c = c0;
+      s.xm = xm0;
+      s.xp = xp0;
+      s.ym = ym0;
+      s.yp = yp0;
+      s.zm = zm0;
+      s.zp = zp0;
+    } else {
+      const float kc = kv(id);
+      const float kxm = 0.5f * (kc + kv(id - 1)), kxp = 0.5f * (kc + kv(id + 1));
+      const float kym = 0.5f * (kc + kv(id - nx)), kyp = 0.5f * (kc + kv(id + nx));
+      s.xm = -kxm * ihx2 - cx;
+      s.xp = -kxp * ihx2 + cx;
+      s.ym = -kym * ihy2 - dyc;
+      s.yp = -kyp * ihy2 + dyc;
+      float c = (kxm + kxp) * ihx2 + (kym + kyp) * ihy2;
+      if (dim == 3) {
+        const float kzm = 0.5f * (kc + kv(id - sxy)), kzp = 0.5f * (kc + kv(id + sxy));
+        s.zm = -kzm * ihz2 - dzc;
+        s.zp = -kzp * ihz2 + dzc;
+        c += (kzm + kzp) * ihz2;
+      } else {
+        s.zm = s.zp = 0.f;
+      }
+      s.c = c + e;
+    }
+    if (i == 1 || i == nx - 2 || j == 1 || j == ny - 2 || (dim == 3 && (kz == 1 || kz == nz - 2)))
+      fold_faces<float>(*g, i, j, kz, s, nullptr);
+    return s;
+  }
+};
+
 __device__ __forceinline__ long long bid(const GridDev& g, int i, int j, int k) {
   return ((long long)k * g.ny + j) * g.nx + i;
 }
@@ -238,6 +314,11 @@ struct BPostRZ {
 // --------------------------------------------------------------- kernels
 
 constexpr int kBThreads = 256;
+// resident blocks per SM asked of the tile kernels (6: a 40-register cap):
+// they are latency-bound, so more warps in flight beat more registers (the
+// smoother takes 8, prolongation and the FP32 apply 5, restriction 4 to
+// avoid spilling)
+constexpr int kBMinBlocks = 6;
 
 // Folded right-hand side b64 = -f - (face shift) and x64 = 0 on level 0.
 __global__ void __launch_bounds__(kBThreads) kb_rhs(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
@@ -311,7 +392,7 @@ __global__ void __launch_bounds__(kBThreads) kb_outer(const BTile* __restrict__ 
 }
 
 // q = A p (FP32 operator, FP32 k), sum p.q in FP64.
-__global__ void __launch_bounds__(kBThreads) kb_apply_pq(const BTile* __restrict__ tiles,
+__global__ void __launch_bounds__(kBThreads, 5) kb_apply_pq(const BTile* __restrict__ tiles,
                                                          const BLevel* __restrict__ lv, BMember* mem,
                                                          double* partials) {
   const BTile T = tiles[blockIdx.x];
@@ -320,18 +401,18 @@ __global__ void __launch_bounds__(kBThreads) kb_apply_pq(const BTile* __restrict
   const BLevel& L = lv[T.lev];
   const float* __restrict__ p = m->p;
   float* __restrict__ q = m->q;
-  const float* k32 = m->k32;
-  const int nx = L.g.nx, dim = L.g.dim;
-  const long long sxy = L.g.sxy;
+  FStencil<float> S;
+  S.load(L, m->k32);
+  const int nx = S.nx, sxy = S.sxy, dim = S.dim;
   const bool is3 = dim == 3;
   double acc[1] = {0.0};
   tile_columns(T, [&](int i, int j) {
-    long long id = bid(L.g, i, j, T.z0);
+    int id = (T.z0 * S.ny + j) * nx + i;
     float zm = is3 ? p[id - sxy] : 0.f;
     float zc = p[id];
     for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
       const float zp = is3 ? p[id + sxy] : 0.f;
-      const Stencil<float> s = bstencil<float, float>(L, k32, i, j, kk, id, nullptr);
+      const Stencil<float> s = S.at(i, j, kk, id);
       const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, dim);
       q[id] = v;
       acc[0] += double(zc) * double(v);
@@ -410,21 +491,21 @@ __global__ void __launch_bounds__(kBThreads) kb_pupdate(const BTile* __restrict_
 // x is taken as zero (first pass of a level): the colour's nodes get b/diag,
 // the other colour's nodes 0.
 template <typename KT>
-__global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+__global__ void __launch_bounds__(kBThreads, 8) kb_smooth(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
                                                        const BMember* mem, int color, int from_zero) {
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
   if (!vcycle_state(bstate(mem + T.member))) return;
   const BLevel& L = lv[T.lev];
-  const KT* k = static_cast<const KT*>(L.kh);
   float* __restrict__ x = L.x;
   // In one colour pass no node is both written and read (updated nodes read
   // only the other colour), so the reads go through a separate read-only
   // view and the loads of later nodes can overlap earlier stores.
   const float* __restrict__ xr = L.x;
   const float* __restrict__ b = L.b;
-  const int nx = L.g.nx, dim = L.g.dim;
-  const long long sxy = L.g.sxy;
+  FStencil<KT> S;
+  S.load(L, static_cast<const KT*>(L.kh));
+  const int nx = S.nx, sxy = S.sxy, dim = S.dim;
   const bool is3 = dim == 3;
   if (!is3 && !from_zero) {
     // 2D: threads walk only the cells of the colour being updated
@@ -437,8 +518,8 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
       const int ra = 2 * c + ((i0 + j + color) & 1);
       if (ra >= int(T.w)) continue;
       const int i = i0 + ra;
-      const long long id = (long long)j * nx + i;
-      const Stencil<float> s = bstencil<float, KT>(L, k, i, j, 0, id, nullptr);
+      const int id = j * nx + i;
+      const Stencil<float> s = S.at(i, j, 0, id);
       x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], 0.f, 0.f, dim)) / s.c;
     }
     return;
@@ -446,9 +527,9 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
   tile_columns(T, [&](int i, int j) {
     if (from_zero) {
       for (int kk = T.z0; kk < T.z1; ++kk) {
-        const long long id = bid(L.g, i, j, kk);
+        const int id = (kk * S.ny + j) * nx + i;
         if (((i + j + kk) & 1) == color) {
-          const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+          const Stencil<float> s = S.at(i, j, kk, id);
           x[id] = b[id] / s.c;
         } else {
           x[id] = 0.f;
@@ -457,8 +538,8 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
     } else {
 #pragma unroll 2
       for (int kk = T.z0 + ((i + j + T.z0 + color) & 1); kk < T.z1; kk += 2) {
-        const long long id = bid(L.g, i, j, kk);
-        const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+        const int id = (kk * S.ny + j) * nx + i;
+        const Stencil<float> s = S.at(i, j, kk, id);
         const float zp = is3 ? xr[id + sxy] : 0.f;
         const float zm = is3 ? xr[id - sxy] : 0.f;
         x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], zp, zm, dim)) / s.c;
@@ -469,26 +550,26 @@ __global__ void __launch_bounds__(kBThreads) kb_smooth(const BTile* __restrict__
 
 // Level residual r = b - A x on level tiles.
 template <typename KT>
-__global__ void __launch_bounds__(kBThreads) kb_residual(const BTile* __restrict__ tiles,
+__global__ void __launch_bounds__(kBThreads, kBMinBlocks) kb_residual(const BTile* __restrict__ tiles,
                                                          const BLevel* __restrict__ lv, const BMember* mem) {
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
   if (!vcycle_state(bstate(mem + T.member))) return;
   const BLevel& L = lv[T.lev];
-  const KT* k = static_cast<const KT*>(L.kh);
   const float* __restrict__ x = L.x;
   const float* __restrict__ b = L.b;
   float* __restrict__ r = L.r;
-  const int nx = L.g.nx, dim = L.g.dim;
-  const long long sxy = L.g.sxy;
+  FStencil<KT> S;
+  S.load(L, static_cast<const KT*>(L.kh));
+  const int nx = S.nx, sxy = S.sxy, dim = S.dim;
   const bool is3 = dim == 3;
   tile_columns(T, [&](int i, int j) {
-    long long id = bid(L.g, i, j, T.z0);
+    int id = (T.z0 * S.ny + j) * nx + i;
     float zm = is3 ? x[id - sxy] : 0.f;
     float zc = x[id];
     for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
       const float zp = is3 ? x[id + sxy] : 0.f;
-      const Stencil<float> s = bstencil<float, KT>(L, k, i, j, kk, id, nullptr);
+      const Stencil<float> s = S.at(i, j, kk, id);
       r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, dim));
       zm = zc;
       zc = zp;
@@ -502,7 +583,7 @@ __global__ void __launch_bounds__(kBThreads) kb_residual(const BTile* __restrict
 constexpr int kBCoarseSmem = 256;
 
 template <typename KT>
-__device__ void bcoarse_solve(const BLevel& C, int sweeps) {
+__device__ __noinline__ void bcoarse_solve(const BLevel& C, int sweeps) {
   __shared__ double cs[kBCoarseSmem];
   const KT* k = static_cast<const KT*>(C.kh);
   const GridDev& g = C.g;
@@ -555,8 +636,66 @@ __device__ void bcoarse_solve(const BLevel& C, int sweeps) {
 // coarse nodes (the boundary-closure fold recomputes the full weight of each
 // Neumann/Robin boundary node that feeds an interior one). A whole-grid tile
 // of a coarsest level then solves that level in the same block.
+// Boundary-closure fold of the restriction at an interior coarse node next to
+// a face: coef x full weight of each boundary node whose chain ends there.
+__device__ __noinline__ double brestrict_fold(const GridDev& gf, const GridDev& gc, const float* __restrict__ rf,
+                                              int I, int J, int K, int dxl, int dxh, int dyl, int dyh, int dzl,
+                                              int dzh) {
+  double fold = 0.0;
+  for (int dk = dzl; dk <= dzh; ++dk)
+    for (int dj = dyl; dj <= dyh; ++dj)
+      for (int di = dxl; di <= dxh; ++di) {
+        if (di == 0 && dj == 0 && dk == 0) continue;
+        int ci = I + di, cj = J + dj, ck = K + dk;
+        const double coef = ext_chain(gc, ci, cj, ck);
+        if (coef != 0.0 && ci == I && cj == J && ck == K)
+          fold += coef * full_weight<float>(gf, gc, rf, I + di, J + dj, K + dk);
+      }
+  return fold;
+}
+
+// One coarse column of the restriction in the general form (any transfer
+// map), out of line so the common nested path keeps few registers.
+__device__ __noinline__ void brestrict_column_general(const BLevel& F, const BLevel& C, const float* __restrict__ rf,
+                                                      float* __restrict__ bc, const BTile& T, int I, int J, int dxl,
+                                                      int dxh, int dyl, int dyh, bool zmarch, bool zsame) {
+  const GridDev& gc = C.g;
+  FwColumn<float> col;
+  col.init(F.g, gc, rf, I, J);
+  // nested z: fine plane 2K+1 feeds coarse planes K and K+1 (sum kept)
+  double below = zmarch && gc.dim == 3 && !zsame ? col.plane(2 * T.z0 - 1) : 0.0;
+  for (int K = T.z0; K < T.z1; ++K) {
+    double acc;
+    if (!zmarch) {
+      acc = full_weight<float>(F.g, gc, rf, I, J, K);
+    } else if (gc.dim != 3) {
+      acc = col.plane(0);
+    } else if (zsame) {
+      acc = col.plane(K);
+    } else {
+      const double mid = col.plane(2 * K);
+      const double above = 2 * K + 1 <= F.g.nz - 1 ? col.plane(2 * K + 1) : 0.0;
+      acc = 0.25 * below + 0.5 * mid + 0.25 * above;
+      below = above;
+    }
+    const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+    if (dxl | dxh | dyl | dyh | dzl | dzh) {
+      for (int dk = dzl; dk <= dzh; ++dk)
+        for (int dj = dyl; dj <= dyh; ++dj)
+          for (int di = dxl; di <= dxh; ++di) {
+            if (di == 0 && dj == 0 && dk == 0) continue;
+            int ci = I + di, cj = J + dj, ck = K + dk;
+            const double coef = ext_chain(gc, ci, cj, ck);
+            if (coef != 0.0 && ci == I && cj == J && ck == K)
+              acc += coef * full_weight<float>(F.g, gc, rf, I + di, J + dj, K + dk);
+          }
+    }
+    bc[bid(gc, I, J, K)] = float(acc);
+  }
+}
+
 template <typename KT>
-__global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict__ tiles,
+__global__ void __launch_bounds__(kBThreads, 4) kb_restrict(const BTile* __restrict__ tiles,
                                                          const BLevel* __restrict__ lv, const BMember* mem,
                                                          int coarse_sweeps) {
   const BTile T = tiles[blockIdx.x];
@@ -604,57 +743,15 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
           below = above;
         }
         const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
-        if (dxl | dxh | dyl | dyh | dzl | dzh) {
-          double fold = 0.0;
-          for (int dk = dzl; dk <= dzh; ++dk)
-            for (int dj = dyl; dj <= dyh; ++dj)
-              for (int di = dxl; di <= dxh; ++di) {
-                if (di == 0 && dj == 0 && dk == 0) continue;
-                int ci = I + di, cj = J + dj, ck = K + dk;
-                const double coef = ext_chain(gc, ci, cj, ck);
-                if (coef != 0.0 && ci == I && cj == J && ck == K)
-                  fold += coef * full_weight<float>(F.g, gc, rf, I + di, J + dj, K + dk);
-              }
-          acc = float(double(acc) + fold);
-        }
+        if (dxl | dxh | dyl | dyh | dzl | dzh)
+          acc = float(double(acc) + brestrict_fold(F.g, gc, rf, I, J, K, dxl, dxh, dyl, dyh, dzl, dzh));
         bc[bid(gc, I, J, K)] = acc;
       }
       return;
     }
     const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
     const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
-    FwColumn<float> col;
-    col.init(F.g, gc, rf, I, J);
-    // nested z: fine plane 2K+1 feeds coarse planes K and K+1 (sum kept)
-    double below = zmarch && gc.dim == 3 && !zsame ? col.plane(2 * T.z0 - 1) : 0.0;
-    for (int K = T.z0; K < T.z1; ++K) {
-      double acc;
-      if (!zmarch) {
-        acc = full_weight<float>(F.g, gc, rf, I, J, K);
-      } else if (gc.dim != 3) {
-        acc = col.plane(0);
-      } else if (zsame) {
-        acc = col.plane(K);
-      } else {
-        const double mid = col.plane(2 * K);
-        const double above = 2 * K + 1 <= F.g.nz - 1 ? col.plane(2 * K + 1) : 0.0;
-        acc = 0.25 * below + 0.5 * mid + 0.25 * above;
-        below = above;
-      }
-      const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
-      if (dxl | dxh | dyl | dyh | dzl | dzh) {
-        for (int dk = dzl; dk <= dzh; ++dk)
-          for (int dj = dyl; dj <= dyh; ++dj)
-            for (int di = dxl; di <= dxh; ++di) {
-              if (di == 0 && dj == 0 && dk == 0) continue;
-              int ci = I + di, cj = J + dj, ck = K + dk;
-              const double coef = ext_chain(gc, ci, cj, ck);
-              if (coef != 0.0 && ci == I && cj == J && ck == K)
-                acc += coef * full_weight<float>(F.g, gc, rf, I + di, J + dj, K + dk);
-            }
-      }
-      bc[bid(gc, I, J, K)] = float(acc);
-    }
+    brestrict_column_general(F, C, rf, bc, T, I, J, dxl, dxh, dyl, dyh, zmarch, zsame);
   });
   if (T.coarse) {
     __syncthreads();
@@ -663,7 +760,7 @@ __global__ void __launch_bounds__(kBThreads) kb_restrict(const BTile* __restrict
 }
 
 // x_l += P Ext(x_{l+1}) on level-l tiles of members with a coarser level.
-__global__ void __launch_bounds__(kBThreads) kb_prolong(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
+__global__ void __launch_bounds__(kBThreads, 5) kb_prolong(const BTile* __restrict__ tiles, const BLevel* __restrict__ lv,
                                                         const BMember* mem) {
   const BTile T = tiles[blockIdx.x];
   if (T.coarse) return;
