@@ -250,9 +250,11 @@ def bench_serving(abi, count=256, seed=7):
     out = {}
     for mode, plist in (("device_resident", dprobs), ("host_inputs", probs)):
         res_mode = {}
-        for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
-            with Server(lanes=4, precision=prec, tile_x=64, tile_y=64, tile_z=32, pre_smooth=1, post_smooth=2,
-                        inner_tol=1e-5) as s:
+        # each precision at its best lane setting on this box: mixed groups of
+        # at most 64 requests on 4 lanes, plain FP64 one request per lane on 8
+        for name, prec, lanes in (("mixed", abi.MIXED, 4), ("fp64", abi.FP64, 8)):
+            with Server(lanes=lanes, max_batch=64, precision=prec, tile_x=64, tile_y=64, tile_z=32, pre_smooth=1,
+                        post_smooth=2, inner_tol=1e-5) as s:
                 dv = mode == "device_resident"
                 s.wait(s.submit_poisson(plist[0], out=outs[0].data_ptr() if dv else None))
                 s.stats(reset=True)
@@ -262,6 +264,7 @@ def bench_serving(abi, count=256, seed=7):
                 wall = time.perf_counter() - t0
                 st = s.stats()
             res_mode[name] = {"solves_per_s": len(plist) / wall, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                              "lanes": lanes,
                               "failed": int(sum(r.status != abi.OK for r in res)),
                               "max_group": int(max(r.group_size for r in res))}
         res_mode["speedup_mixed_vs_fp64"] = res_mode["mixed"]["solves_per_s"] / res_mode["fp64"]["solves_per_s"]

@@ -38,7 +38,8 @@ typedef enum {
 typedef struct {
   int32_t device;
   int32_t lanes;             /* concurrent lanes (streams); 0 = 4 */
-  int32_t max_batch;         /* Poisson requests per batched group; 0 = 256 */
+  int32_t max_batch;         /* Poisson requests per batched group; 0 = 64 (groups on several lanes
+                                overlap one group's last, sparse cycles with another's full ones) */
   int32_t precision;         /* PDEB200_MIXED (batched groups) or PDEB200_FP64 (plain MG-PCG path) */
   int64_t hbm_budget_bytes;  /* admission budget; 0 = 80% of the device's free memory at create */
   int32_t queue_capacity;    /* queued (not yet admitted) requests; 0 = 65536 */

@@ -62,7 +62,7 @@ struct SReq {
 struct Server {
   int dev = 0;
   int nlanes = 4;
-  int max_batch = 256;
+  int max_batch = 64;
   int precision = PDEB200_MIXED;
   int queue_cap = 65536;
   int64_t budget = 0;
@@ -330,7 +330,7 @@ pdeb200_status pdeb200_server_create(const pdeb200_server_options* opt, pdeb200_
     Server& S = h->s;
     S.dev = opt->device;
     S.nlanes = opt->lanes > 0 ? opt->lanes : 4;
-    S.max_batch = opt->max_batch > 0 ? opt->max_batch : 256;
+    S.max_batch = opt->max_batch > 0 ? opt->max_batch : 64;
     S.precision = opt->precision == PDEB200_FP64 ? PDEB200_FP64 : PDEB200_MIXED;
     S.queue_cap = opt->queue_capacity > 0 ? opt->queue_capacity : 65536;
     S.bopt = opt->batch;

@@ -29,7 +29,7 @@ def _dp(a):
 
 
 class Server:
-    def __init__(self, lanes=4, max_batch=256, precision=abi.MIXED, hbm_budget_bytes=0, device=0,
+    def __init__(self, lanes=4, max_batch=64, precision=abi.MIXED, hbm_budget_bytes=0, device=0,
                  queue_capacity=0, **batch_kw):
         self.lib = abi.load()
         o = abi.ServerOptions()
