@@ -318,6 +318,33 @@ pdeb200_status pdeb200_jacobi_noalloc(const pdeb200_problem* prob, int32_t max_i
                                       int32_t device, void* stream, double* out_grid,
                                       pdeb200_report* report);
 
+/* ---- expressions of x, y, z, t on the grid ----------------------------- */
+
+/* Fills out[(k*ny + j)*nx + i] with the LaTeX expression evaluated at node
+ * (xmin + i*dx, ymin + j*dy, zmin + k*dz) and time t, on the GPU. Replaces the
+ * reference's per-node host loops over ExpressionEvaluator::Eval
+ * (src/expression_eval.cpp:805-978; called per node from
+ * src/backends/cpu/solver.cpp:197 for the right side and
+ * src/backends/cpu/cpu_utils.cpp:520-530 for variable coefficients). Same
+ * language as ExpressionEvaluator::ParseLatex: \frac, \sqrt, \cdot, \times,
+ * \pi, \theta, \phi, \left/\right, \operatorname{}, the one-argument
+ * functions sin ... erf (ln, arcsin, arccos, arctan, sgn as aliases), min,
+ * max, atan2, pow; x/r, y/theta, z/phi, t, pi, e; implicit multiplication;
+ * guarded division, powers, logarithms and roots that give NaN where the
+ * reference does. Only the geometry of `grid` (nx, ny, nz, bounds) is used;
+ * nz <= 1 gives z = 0. `out` is a host array of N doubles, or a device
+ * pointer when mem_space is PDEB200_MEM_DEVICE. A parse error returns
+ * PDEB200_ERR_INVALID with the reference's message in `message`. */
+pdeb200_status pdeb200_eval_expression(const char* latex, const pdeb200_problem* grid, double t,
+                                       int32_t device, double* out, int32_t mem_space,
+                                       char* message, size_t message_len);
+
+/* The same compiled expression evaluated once on the host (no GPU), for
+ * checking the compiler against ExpressionEvaluator. */
+pdeb200_status pdeb200_expression_value(const char* latex, double x, double y, double z,
+                                        double t, double* value, char* message,
+                                        size_t message_len);
+
 #ifdef __cplusplus
 }
 #endif

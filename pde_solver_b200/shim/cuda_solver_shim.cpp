@@ -9,11 +9,14 @@
 // compiled inside pde_solver's build (it includes the reference's own
 // pde_types.h and expression_eval.h) and linked against libpdeb200.so. It turns
 // the parsed SolveInput into the POD problem of include/pdeb200.h: LaTeX right
-// sides, coefficients and boundary expressions are evaluated at every node with
-// the reference's ExpressionEvaluator, exactly as the reference's CPU solver
-// evaluates them per node (src/backends/cpu/solver.cpp:197, :834,
-// cpu_utils.cpp:520-530), then one C-ABI call solves on the GPU. Errors come
-// back as SolveOutput.error strings, as the reference's backends report them.
+// sides and coefficients are compiled once and evaluated at every node on the
+// GPU (pdeb200_eval_expression, the language of ExpressionEvaluator), where the
+// reference's CPU solver interprets them node by node
+// (src/backends/cpu/solver.cpp:197, :834); boundary expressions, a few nodes
+// per face with the linear fallback of EvalExpr (cpu_utils.cpp:520-530), use
+// the reference's ExpressionEvaluator on the host. Then one C-ABI call solves
+// on the GPU. Errors come back as SolveOutput.error strings, as the reference's
+// backends report them.
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -81,7 +84,23 @@ bool Unsupported(const SolveInput& in, std::string* why) {
   return false;
 }
 
-bool Materialise(const SolveInput& in, Materialised* m) {
+// A LaTeX field at every node, compiled once and evaluated on the GPU by
+// pdeb200_eval_expression (same language, guards and node coordinates as
+// ExpressionEvaluator::Eval per node). Parse errors carry the reference's
+// message after `prefix`.
+bool EvalOnGrid(const std::string& latex, const pdeb200_problem& grid, int device, double* out, const char* prefix,
+                std::string* error) {
+  char msg[256];
+  const pdeb200_status st = pdeb200_eval_expression(latex.c_str(), &grid, 0.0, device, out, PDEB200_MEM_HOST, msg,
+                                                    sizeof(msg));
+  if (st == PDEB200_OK) return true;
+  *error = st == PDEB200_ERR_INVALID ? std::string(prefix) + msg
+                                     : std::string("B200 expression evaluation failed: ") + pdeb200_status_string(st) +
+                                           (msg[0] ? std::string(" (") + msg + ")" : std::string());
+  return false;
+}
+
+bool Materialise(const SolveInput& in, Materialised* m, int device) {
   const Domain& d = in.domain;
   pdeb200_problem& p = m->prob;
   std::memset(&p, 0, sizeof(p));
@@ -124,17 +143,8 @@ bool Materialise(const SolveInput& in, Materialised* m) {
   };
   // right side (BuildRhs2D / the 3D sweep evaluate it per node)
   if (!in.pde.rhs_latex.empty()) {
-    ExpressionEvaluator ev = ExpressionEvaluator::ParseLatex(in.pde.rhs_latex);
-    if (!ev.ok()) {
-      m->error = "invalid RHS expression: " + ev.error();
-      return false;
-    }
     m->f.resize(n);
-    for (long long id = 0; id < n; ++id) {
-      double x, y, z;
-      node(id, &x, &y, &z);
-      m->f[id] = ev.Eval(x, y, z, 0.0);
-    }
+    if (!EvalOnGrid(in.pde.rhs_latex, p, device, m->f.data(), "invalid RHS expression: ", &m->error)) return false;
     p.f = m->f.data();
   }
   // variable coefficients (EvalCoefficient, src/coefficient_evaluator.cpp:99-105)
@@ -148,16 +158,8 @@ bool Materialise(const SolveInput& in, Materialised* m) {
         std::fill(m->nodal.begin() + q * n, m->nodal.begin() + (q + 1) * n, cst[q]);
         continue;
       }
-      ExpressionEvaluator ev = ExpressionEvaluator::ParseLatex(*lat[q]);
-      if (!ev.ok()) {
-        m->error = "invalid coefficient expression: " + ev.error();
+      if (!EvalOnGrid(*lat[q], p, device, m->nodal.data() + q * n, "invalid coefficient expression: ", &m->error))
         return false;
-      }
-      for (long long id = 0; id < n; ++id) {
-        double x, y, z;
-        node(id, &x, &y, &z);
-        m->nodal[q * n + id] = ev.Eval(x, y, z, 0.0);
-      }
     }
     p.coef_kind = PDEB200_COEF_NODAL;
     p.nodal = m->nodal.data();
@@ -261,7 +263,7 @@ SolveOutput SolvePDECuda(const SolveInput& input) {
   std::string note;
   if (!CudaIsAvailable(&note)) return {"CUDA unavailable: " + note, {}};
   Materialised m;
-  if (!Materialise(input, &m)) return {m.error, {}};
+  if (!Materialise(input, &m, 0)) return {m.error, {}};
   pdeb200_options o;
   FillOptions(input, &o);
   const bool krylov = input.solver.method == SolveMethod::CG || input.solver.method == SolveMethod::BiCGStab ||
@@ -291,7 +293,7 @@ SolveOutput SolvePDETimeSeriesCuda(const SolveInput& input, const FrameCallback&
   if (input.time.integrator != TimeIntegrator::ForwardEuler)
     return {"B200 time series supports forward Euler", {}};
   Materialised m;
-  if (!Materialise(input, &m)) return {m.error, {}};
+  if (!Materialise(input, &m, 0)) return {m.error, {}};
   pdeb200_time_options t{};
   t.t_start = input.time.t_start;
   t.dt = input.time.dt;

@@ -72,6 +72,37 @@ def residual_norms(problem: GridProblem, grid, device: int = 0):
     return l2.value, linf.value
 
 
+def eval_expression(latex: str, problem: GridProblem, t: float = 0.0, device: int = 0, out=None):
+    """The LaTeX expression at every node of `problem`'s grid, computed on the
+    GPU (ExpressionEvaluator::Eval per node, src/expression_eval.cpp:841-978).
+    Host array result unless `out` is a device pointer (int)."""
+    lib = _lib()
+    cp = problem.to_c()
+    msg = C.create_string_buffer(256)
+    if out is not None and not isinstance(out, np.ndarray):
+        st = lib.pdeb200_eval_expression(latex.encode(), C.byref(cp), t, device, C.c_void_p(out), abi.MEM_DEVICE,
+                                         msg, 256)
+        res = out
+    else:
+        res = np.empty(problem.n) if out is None else out
+        st = lib.pdeb200_eval_expression(latex.encode(), C.byref(cp), t, device, res.ctypes.data_as(C.c_void_p),
+                                         abi.MEM_HOST, msg, 256)
+    if st != abi.OK:
+        raise SolveError(st, msg.value.decode() or lib.pdeb200_status_string(st).decode())
+    return res
+
+
+def expression_value(latex: str, x: float, y: float, z: float = 0.0, t: float = 0.0) -> float:
+    """One host evaluation of the compiled expression (no GPU needed)."""
+    lib = _lib()
+    v = C.c_double()
+    msg = C.create_string_buffer(256)
+    st = lib.pdeb200_expression_value(latex.encode(), x, y, z, t, C.byref(v), msg, 256)
+    if st != abi.OK:
+        raise SolveError(st, msg.value.decode())
+    return v.value
+
+
 def time_series(problem: GridProblem, t_start: float, dt: float, frames: int, on_frame=None, device: int = 0,
                 frame_stride: int = 1):
     """Forward-Euler frames (SolvePDETimeSeries). on_frame(frame, t, grid) -> bool."""

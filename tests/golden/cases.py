@@ -71,3 +71,73 @@ def residual_case():
                FaceBC.dirichlet(1.0), FaceBC(), FaceBC()]
     grid = np.random.Generator(np.random.PCG64(3)).standard_normal(p.n)
     return p, grid
+
+
+def expression_cases():
+    """LaTeX expressions with the grid and time they are evaluated on:
+    (latex, nx, ny, nz, bounds, t). They cover every command, function, alias,
+    constant and guard of the reference's evaluator (src/expression_eval.cpp)."""
+    b2 = (-1.0, 1.0, -0.5, 1.5, 0.0, 0.0)
+    b3 = (0.0, 1.0, -1.0, 1.0, 0.25, 2.0)
+    pos = (0.1, 2.0, 0.2, 3.0, 0.0, 0.0)
+    return [
+        (r"\sin(\pi*x)\sin(\pi*y)", 17, 13, 1, b2, 0.0),
+        (r"-2\pi^2\sin(\pi*x)\cdot\sin(\pi*y)", 17, 13, 1, b2, 0.0),
+        (r"\frac{x^2 + y^2}{1 + x^2}", 17, 13, 1, b2, 0.0),
+        (r"\sqrt{x^2+y^2+z^2} \times e^{-t}", 9, 7, 5, b3, 0.75),
+        (r"\exp(-(x^2+y^2)/0.1)", 17, 13, 1, b2, 0.0),
+        (r"\left(x + 1\right)^{3} - 2 x", 17, 13, 1, b2, 0.0),
+        (r"2(x)(y) + 3y\cdot z\,", 9, 7, 5, b3, 0.0),
+        (r"x^y^2", 17, 13, 1, pos, 0.0),
+        (r"-x^2", 17, 13, 1, b2, 0.0),
+        (r"\tan(x) + \tanh(y) + \sinh(x) - \cosh(y)", 17, 13, 1, b2, 0.0),
+        (r"\arcsin(x) + \arccos(y) + \arctan(x*y)", 17, 13, 1, b2, 0.0),
+        (r"\operatorname{asin}(2x) + \operatorname{acos}(y/2)", 17, 13, 1, b2, 0.0),
+        (r"\ln(x) + \log{y}", 17, 13, 1, b2, 0.0),
+        (r"\ln(x) + \log{y}", 17, 13, 1, pos, 0.0),
+        (r"\sqrt{x}", 17, 13, 1, b2, 0.0),
+        (r"\frac{1}{x}", 17, 13, 1, b2, 0.0),
+        (r"\frac{1}{x - y}", 17, 17, 1, (0.0, 1.0, 0.0, 1.0, 0.0, 0.0), 0.0),
+        (r"\exp(800 x) + \exp(-800 x)", 17, 13, 1, b2, 0.0),
+        (r"\floor(4x) + \ceil(4y) + \round(2.5x) + \abs(x\cdot y)", 17, 13, 1, b2, 0.0),
+        (r"\sign(x) + \sgn{y} + \operatorname{sgn}(x+y)", 17, 13, 1, b2, 0.0),
+        (r"\erf(x) \cdot \erf(2y)", 17, 13, 1, b2, 0.0),
+        (r"\min{x,y} + \max(x, y^2)", 17, 13, 1, b2, 0.0),
+        (r"\pow{x, 2} + \pow(y, 0.5) + \operatorname{pow}{x, y}", 17, 13, 1, b2, 0.0),
+        (r"x^{0.5} + (-2)^{3} + (-8)^{1/3}", 17, 13, 1, b2, 0.0),
+        (r"\sin{\pi} + \cos\pi + \sin x + \cos 2 + \exp .5", 17, 13, 1, b2, 0.0),
+        (r"r\cdot\cos(\theta) + \phi + \vartheta*\varphi", 9, 7, 5, b3, 0.0),
+        (r"$x + t$", 17, 13, 1, b2, 1.25),
+        (r"\sin(x)^2 + \cos(x)^2", 17, 13, 1, b2, 0.0),
+        (r"e^{x} - e", 17, 13, 1, b2, 0.0),
+        (r"1.5e-3 + .25 + 3.", 17, 13, 1, b2, 0.0),
+        (r"f(x) + 1", 17, 13, 1, b2, 0.0),
+        (r"+-+x", 17, 13, 1, b2, 0.0),
+        (r"\frac{\sin(\pi*x)}{\pi*(1 + t)}\frac{y}{2}", 9, 7, 5, b3, 2.0),
+    ]
+
+
+def expression_errors():
+    """Expressions the reference rejects; the message must match."""
+    return [
+        r"\sin(\pi x)",
+        r"2xy",
+        r"\foo(x)",
+        r"\frac{1}",
+        r"\sqrt(x)",
+        r"\min{x}",
+        r"x + }",
+        r"(x + 1",
+        r"x + ",
+        r"x $ # y",
+        r"",
+        r"\left(\right)",
+        r"\sin",
+        r"\sin\,",
+        "(" * 60 + "x" + ")" * 60,
+        "-" * 120 + "x",
+        r"\max{x,",
+        r"3y\,z",
+        r"\atan2{y, x}",
+        r"\operatorname{atan2}{y, x}",
+    ]
