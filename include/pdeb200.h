@@ -339,6 +339,20 @@ pdeb200_status pdeb200_eval_expression(const char* latex, const pdeb200_problem*
                                        int32_t device, double* out, int32_t mem_space,
                                        char* message, size_t message_len);
 
+/* One boundary expression on the nodes of one face (0..5 = left, right,
+ * bottom, top, front, back), in the face-local order of pdeb200_face arrays,
+ * with the reference's EvalExpr rule (src/backends/cpu/cpu_utils.cpp:520-530):
+ * the LaTeX value where `latex` parses and the value is finite, else the
+ * linear form linear[0] + linear[1]*x + linear[2]*y + linear[3]*z
+ * (BoundaryCondition::Expression, include/pde_types.h). `latex` may be NULL
+ * or empty, and an expression that does not parse is not an error (the
+ * linear form is used), as in the reference. `linear` may be NULL (zeros).
+ * Faces 4 and 5 need nz > 1. */
+pdeb200_status pdeb200_eval_face_expression(const char* latex, const double* linear,
+                                            const pdeb200_problem* grid, int32_t face, double t,
+                                            int32_t device, double* out, int32_t mem_space,
+                                            char* message, size_t message_len);
+
 /* The same compiled expression evaluated once on the host (no GPU), for
  * checking the compiler against ExpressionEvaluator. */
 pdeb200_status pdeb200_expression_value(const char* latex, double x, double y, double z,

@@ -330,6 +330,9 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_eval_expression.restype = C.c_int32
     lib.pdeb200_eval_expression.argtypes = [C.c_char_p, P(Problem), C.c_double, C.c_int32, C.c_void_p, C.c_int32,
                                             C.c_char_p, C.c_size_t]
+    lib.pdeb200_eval_face_expression.restype = C.c_int32
+    lib.pdeb200_eval_face_expression.argtypes = [C.c_char_p, P(C.c_double), P(Problem), C.c_int32, C.c_double,
+                                                 C.c_int32, C.c_void_p, C.c_int32, C.c_char_p, C.c_size_t]
     lib.pdeb200_expression_value.restype = C.c_int32
     lib.pdeb200_expression_value.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double,
                                              P(C.c_double), C.c_char_p, C.c_size_t]

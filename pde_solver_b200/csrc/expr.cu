@@ -125,9 +125,28 @@ __host__ __device__ inline double expr_run(const ExprProg& P, double x, double y
   return sp > 0 ? st[sp - 1] : 0.0;
 }
 
-// Node coordinates x = min + i*h, unfused as on the host.
-__global__ void k_eval_expr(const ExprProg* __restrict__ prog, int nx, int ny, long long n, double x0, double y0,
-                            double z0, double dx, double dy, double dz, double t, double* __restrict__ out) {
+// Where the nodes of a launch sit: the launch walks an (na, nb, nc) index box
+// (a fastest) and each coordinate is either base + index*step for one of the
+// three indices (unfused, as the host computes min + i*h) or the fixed base.
+struct NodeMap {
+  int na, nb;
+  int axis[3];     // 0, 1, 2: index a, b, c; 3: fixed at base
+  double base[3];
+  double step[3];
+  int has_prog;    // 0: no expression, the linear form alone
+  int linear;      // 1: non-finite values fall back to the linear form
+  double lin[4];   // constant, x, y, z coefficients of the linear form
+};
+
+__device__ inline double node_coord(const NodeMap& m, int c, int a, int b, int k) {
+  const int ax = m.axis[c];
+  if (ax == 3) return m.base[c];
+  const int idx = ax == 0 ? a : (ax == 1 ? b : k);
+  return __dadd_rn(m.base[c], __dmul_rn(double(idx), m.step[c]));
+}
+
+__global__ void k_eval_expr(const ExprProg* __restrict__ prog, NodeMap m, long long n, double t,
+                            double* __restrict__ out) {
   __shared__ ExprProg P;
   {
     const int* s = reinterpret_cast<const int*>(prog);
@@ -137,12 +156,16 @@ __global__ void k_eval_expr(const ExprProg* __restrict__ prog, int nx, int ny, l
   __syncthreads();
   for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += (long long)gridDim.x * blockDim.x) {
-    const int i = int(id % nx), j = int((id / nx) % ny);
-    const int k = int(id / ((long long)nx * ny));
-    const double x = __dadd_rn(x0, __dmul_rn(double(i), dx));
-    const double y = __dadd_rn(y0, __dmul_rn(double(j), dy));
-    const double z = __dadd_rn(z0, __dmul_rn(double(k), dz));
-    out[id] = expr_run(P, x, y, z, t);
+    const int a = int(id % m.na), b = int((id / m.na) % m.nb);
+    const int k = int(id / ((long long)m.na * m.nb));
+    const double x = node_coord(m, 0, a, b, k);
+    const double y = node_coord(m, 1, a, b, k);
+    const double z = node_coord(m, 2, a, b, k);
+    double v = m.has_prog ? expr_run(P, x, y, z, t) : nan("");
+    if (m.linear && !isfinite(v))
+      v = __dadd_rn(__dadd_rn(__dadd_rn(m.lin[0], __dmul_rn(m.lin[1], x)), __dmul_rn(m.lin[2], y)),
+                    __dmul_rn(m.lin[3], z));
+    out[id] = v;
   }
 }
 
@@ -515,6 +538,72 @@ void copy_msg(char* dst, size_t len, const std::string& m) {
   dst[len - 1] = '\0';
 }
 
+// Node map of the whole grid (face < 0) or of one face in the face-local
+// order of pdeb200_face arrays: left/right j + ny*k, bottom/top i + nx*k,
+// front/back i + nx*j. 2D grids have z = 0.
+pdeb200_status grid_map(const pdeb200_problem* g, int face, NodeMap* m, long long* n) {
+  const int nz = g->nz > 1 ? g->nz : 1;
+  if (g->nx < 2 || g->ny < 2 || (face >= 4 && nz < 2)) return PDEB200_ERR_INVALID;
+  const double dx = (g->xmax - g->xmin) / (g->nx - 1);
+  const double dy = (g->ymax - g->ymin) / (g->ny - 1);
+  const double dz = nz > 1 ? (g->zmax - g->zmin) / (nz - 1) : 0.0;
+  const double lo[3] = {g->xmin, g->ymin, nz > 1 ? g->zmin : 0.0};
+  const double hi[3] = {g->xmax, g->ymax, nz > 1 ? g->zmax : 0.0};
+  const double h[3] = {dx, dy, dz};
+  const int dims[3] = {g->nx, g->ny, nz};
+  int fixed = face < 0 ? -1 : face / 2;  // axis held at a boundary value
+  int idx = 0, sizes[3] = {1, 1, 1};
+  for (int c = 0; c < 3; ++c) {
+    m->base[c] = lo[c];
+    m->step[c] = h[c];
+    if (c == fixed) {
+      m->axis[c] = 3;
+      m->base[c] = (face & 1) ? hi[c] : lo[c];
+    } else if (c == 2 && nz == 1) {
+      m->axis[c] = 3;
+      m->base[c] = 0.0;
+    } else {
+      m->axis[c] = idx;
+      sizes[idx++] = dims[c];
+    }
+  }
+  m->na = sizes[0];
+  m->nb = sizes[1];
+  *n = (long long)sizes[0] * sizes[1] * sizes[2];
+  return PDEB200_OK;
+}
+
+pdeb200_status run_eval(const ExprProg* P, const NodeMap& m, long long n, double t, int device, double* out,
+                        int mem_space, char* message, size_t message_len) {
+  try {
+    Context* ctx = get_context(device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Buf prog(sizeof(ExprProg), ctx->stream);
+    PDEB_CUDA(cudaMemcpyAsync(prog.as<void>(), P, sizeof(ExprProg), cudaMemcpyHostToDevice, ctx->stream));
+    double* d_out = out;
+    Buf ob;
+    if (mem_space != PDEB200_MEM_DEVICE) {
+      ob = Buf(sizeof(double) * n, ctx->stream);
+      d_out = ob.as<double>();
+    }
+    const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->num_sms * 16);
+    k_eval_expr<<<blocks, 256, 0, ctx->stream>>>(prog.as<ExprProg>(), m, n, t, d_out);
+    PDEB_CUDA(cudaGetLastError());
+    ctx->count();
+    if (mem_space != PDEB200_MEM_DEVICE)
+      PDEB_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
+  } catch (const StatusFailure& s) {
+    copy_msg(message, message_len, s.what);
+    return s.status;
+  } catch (const CudaFailure& c) {
+    copy_msg(message, message_len, c.what);
+    cudaGetLastError();
+    return PDEB200_ERR_CUDA;
+  }
+  return PDEB200_OK;
+}
+
 }  // namespace
 }  // namespace pdeb
 
@@ -541,11 +630,6 @@ pdeb200_status pdeb200_eval_expression(const char* latex, const pdeb200_problem*
   using namespace pdeb;
   copy_msg(message, message_len, "");
   if (!latex || !grid || !out) return PDEB200_ERR_INVALID;
-  const int nz = grid->nz > 1 ? grid->nz : 1;
-  if (grid->nx < 2 || grid->ny < 2) {
-    copy_msg(message, message_len, "grid must have at least 2 nodes per dimension");
-    return PDEB200_ERR_INVALID;
-  }
   auto P = std::make_unique<ExprProg>();
   try {
     compile(latex, P.get());
@@ -553,38 +637,45 @@ pdeb200_status pdeb200_eval_expression(const char* latex, const pdeb200_problem*
     copy_msg(message, message_len, f.what);
     return PDEB200_ERR_INVALID;
   }
-  const long long n = (long long)grid->nx * grid->ny * nz;
-  const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
-  const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
-  const double dz = nz > 1 ? (grid->zmax - grid->zmin) / (nz - 1) : 0.0;
-  const double z0 = nz > 1 ? grid->zmin : 0.0;
-  try {
-    Context* ctx = get_context(device);
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    Buf prog(sizeof(ExprProg), ctx->stream);
-    PDEB_CUDA(cudaMemcpyAsync(prog.as<void>(), P.get(), sizeof(ExprProg), cudaMemcpyHostToDevice, ctx->stream));
-    double* d_out = out;
-    Buf ob;
-    if (mem_space != PDEB200_MEM_DEVICE) {
-      ob = Buf(sizeof(double) * n, ctx->stream);
-      d_out = ob.as<double>();
-    }
-    const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->num_sms * 16);
-    k_eval_expr<<<blocks, 256, 0, ctx->stream>>>(prog.as<ExprProg>(), grid->nx, grid->ny, n, grid->xmin, grid->ymin,
-                                                 z0, dx, dy, dz, t, d_out);
-    PDEB_CUDA(cudaGetLastError());
-    if (mem_space != PDEB200_MEM_DEVICE)
-      PDEB_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    PDEB_CUDA(cudaStreamSynchronize(ctx->stream));
-  } catch (const StatusFailure& s) {
-    copy_msg(message, message_len, s.what);
-    return s.status;
-  } catch (const CudaFailure& c) {
-    copy_msg(message, message_len, c.what);
-    cudaGetLastError();
-    return PDEB200_ERR_CUDA;
+  NodeMap m{};
+  long long n = 0;
+  pdeb200_status st = grid_map(grid, -1, &m, &n);
+  if (st != PDEB200_OK) {
+    copy_msg(message, message_len, "grid must have at least 2 nodes per dimension");
+    return st;
   }
-  return PDEB200_OK;
+  m.has_prog = 1;
+  return run_eval(P.get(), m, n, t, device, out, mem_space, message, message_len);
+}
+
+pdeb200_status pdeb200_eval_face_expression(const char* latex, const double* linear, const pdeb200_problem* grid,
+                                            int32_t face, double t, int32_t device, double* out, int32_t mem_space,
+                                            char* message, size_t message_len) {
+  using namespace pdeb;
+  copy_msg(message, message_len, "");
+  if (!grid || !out || face < 0 || face > 5) return PDEB200_ERR_INVALID;
+  auto P = std::make_unique<ExprProg>();
+  P->n = 0;
+  bool parsed = false;
+  if (latex && latex[0]) {
+    try {
+      compile(latex, P.get());
+      parsed = true;
+    } catch (const Failure&) {
+      P->n = 0;  // an expression that does not parse leaves the linear form
+    }
+  }
+  NodeMap m{};
+  long long n = 0;
+  pdeb200_status st = grid_map(grid, face, &m, &n);
+  if (st != PDEB200_OK) {
+    copy_msg(message, message_len, "grid must have at least 2 nodes per dimension (3D faces need nz > 1)");
+    return st;
+  }
+  m.has_prog = parsed ? 1 : 0;
+  m.linear = 1;
+  for (int q = 0; q < 4; ++q) m.lin[q] = linear ? linear[q] : 0.0;
+  return run_eval(P.get(), m, n, t, device, out, mem_space, message, message_len);
 }
 
 }  // extern "C"

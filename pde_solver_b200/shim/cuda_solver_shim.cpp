@@ -12,10 +12,9 @@
 // sides and coefficients are compiled once and evaluated at every node on the
 // GPU (pdeb200_eval_expression, the language of ExpressionEvaluator), where the
 // reference's CPU solver interprets them node by node
-// (src/backends/cpu/solver.cpp:197, :834); boundary expressions, a few nodes
-// per face with the linear fallback of EvalExpr (cpu_utils.cpp:520-530), use
-// the reference's ExpressionEvaluator on the host. Then one C-ABI call solves
-// on the GPU. Errors come back as SolveOutput.error strings, as the reference's
+// (src/backends/cpu/solver.cpp:197, :834); boundary expressions go through
+// the face form of the same evaluator, with the linear fallback of EvalExpr
+// (cpu_utils.cpp:520-530). Then one C-ABI call solves on the GPU. Errors come back as SolveOutput.error strings, as the reference's
 // backends report them.
 #include <cmath>
 #include <cstring>
@@ -24,7 +23,6 @@
 #include <vector>
 
 #include "cuda_solver.h"
-#include "expression_eval.h"
 #include "pde_types.h"
 #include "pdeb200.h"
 #include "progress.h"
@@ -40,17 +38,6 @@ struct Materialised {
   std::vector<double> face_arr[6][4];
   std::string error;
 };
-
-// EvalExpr of the reference solver (cpu_utils.cpp:520-530): the LaTeX form when
-// it parses and gives a finite value, else the linear form.
-double EvalBcExpr(const BoundaryCondition::Expression& e, const ExpressionEvaluator* ev, double x, double y,
-                  double z, double t) {
-  if (ev && ev->ok()) {
-    const double v = ev->Eval(x, y, z, t);
-    if (std::isfinite(v)) return v;
-  }
-  return e.constant + e.x * x + e.y * y + e.z * z;
-}
 
 bool Unsupported(const SolveInput& in, std::string* why) {
   if (in.domain.coord_system != CoordinateSystem::Cartesian) {
@@ -133,14 +120,6 @@ bool Materialise(const SolveInput& in, Materialised* m, int device) {
   }
   const int nz = p.nz;
   const long long n = (long long)p.nx * p.ny * nz;
-  const double dx = (d.xmax - d.xmin) / (p.nx - 1), dy = (d.ymax - d.ymin) / (p.ny - 1);
-  const double dz = nz > 1 ? (d.zmax - d.zmin) / (nz - 1) : 0.0;
-  auto node = [&](long long id, double* x, double* y, double* z) {
-    const int i = int(id % p.nx), j = int((id / p.nx) % p.ny), k = int(id / ((long long)p.nx * p.ny));
-    *x = d.xmin + i * dx;
-    *y = d.ymin + j * dy;
-    *z = nz > 1 ? d.zmin + k * dz : 0.0;
-  };
   // right side (BuildRhs2D / the 3D sweep evaluate it per node)
   if (!in.pde.rhs_latex.empty()) {
     m->f.resize(n);
@@ -179,28 +158,17 @@ bool Materialise(const SolveInput& in, Materialised* m, int device) {
     const BoundaryCondition::Expression* ex[4] = {&bc.value, &bc.alpha, &bc.beta, &bc.gamma};
     const int w = f <= 1 ? p.ny : p.nx, h = f <= 3 ? nz : p.ny;
     for (int q = 0; q < 4; ++q) {
-      ExpressionEvaluator ev = ExpressionEvaluator::ParseLatex(ex[q]->latex.empty() ? "0" : ex[q]->latex);
-      const ExpressionEvaluator* evp = ex[q]->latex.empty() ? nullptr : &ev;
       std::vector<double>& arr = m->face_arr[f][q];
       arr.resize((size_t)w * h);
-      for (int b = 0; b < h; ++b)
-        for (int a = 0; a < w; ++a) {
-          double x, y, z;
-          if (f <= 1) {
-            x = f == 0 ? d.xmin : d.xmax;
-            y = d.ymin + a * dy;
-            z = nz > 1 ? d.zmin + b * dz : 0.0;
-          } else if (f <= 3) {
-            x = d.xmin + a * dx;
-            y = f == 2 ? d.ymin : d.ymax;
-            z = nz > 1 ? d.zmin + b * dz : 0.0;
-          } else {
-            x = d.xmin + a * dx;
-            y = d.ymin + b * dy;
-            z = f == 4 ? d.zmin : d.zmax;
-          }
-          arr[(size_t)b * w + a] = EvalBcExpr(*ex[q], evp, x, y, z, 0.0);
-        }
+      const double lin[4] = {ex[q]->constant, ex[q]->x, ex[q]->y, ex[q]->z};
+      char msg[256];
+      const pdeb200_status st = pdeb200_eval_face_expression(ex[q]->latex.c_str(), lin, &p, f, 0.0, device,
+                                                             arr.data(), PDEB200_MEM_HOST, msg, sizeof(msg));
+      if (st != PDEB200_OK) {
+        m->error = std::string("B200 boundary evaluation failed: ") + pdeb200_status_string(st) +
+                   (msg[0] ? std::string(" (") + msg + ")" : std::string());
+        return false;
+      }
     }
     F.value_arr = m->face_arr[f][0].data();
     F.alpha_arr = m->face_arr[f][1].data();

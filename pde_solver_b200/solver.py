@@ -92,6 +92,25 @@ def eval_expression(latex: str, problem: GridProblem, t: float = 0.0, device: in
     return res
 
 
+def eval_face_expression(latex: str | None, problem: GridProblem, face: int, linear=(0.0, 0.0, 0.0, 0.0),
+                         t: float = 0.0, device: int = 0):
+    """A boundary expression on the nodes of one face in pdeb200_face order,
+    with the reference's EvalExpr fallback to the linear form
+    (src/backends/cpu/cpu_utils.cpp:520-530)."""
+    lib = _lib()
+    cp = problem.to_c()
+    msg = C.create_string_buffer(256)
+    nx, ny, nz = problem.nx, problem.ny, max(problem.nz, 1)
+    n = (ny * nz) if face <= 1 else (nx * nz if face <= 3 else nx * ny)
+    res = np.empty(n)
+    lin = (C.c_double * 4)(*[float(v) for v in linear])
+    st = lib.pdeb200_eval_face_expression(latex.encode() if latex is not None else None, lin, C.byref(cp), face, t,
+                                          device, res.ctypes.data_as(C.c_void_p), abi.MEM_HOST, msg, 256)
+    if st != abi.OK:
+        raise SolveError(st, msg.value.decode() or lib.pdeb200_status_string(st).decode())
+    return res
+
+
 def expression_value(latex: str, x: float, y: float, z: float = 0.0, t: float = 0.0) -> float:
     """One host evaluation of the compiled expression (no GPU needed)."""
     lib = _lib()

@@ -134,3 +134,47 @@ def test_gpu_large_grid_sampled(lib):
         i, j, k = q % 257, (q // 257) % 257, q // (257 * 257)
         ref = solver.expression_value(latex, i * h, j * h, k * h)
         assert abs(got[q] - ref) <= 1e-13 * abs(ref) + 1e-14 * 3 * np.pi**2
+
+
+def _face_nodes(face, nx, ny, nz, b):
+    """Face-local nodes in pdeb200_face order, coordinates as the reference computes them."""
+    nzz = nz if nz > 1 else 1
+    dx = (b[1] - b[0]) / (nx - 1)
+    dy = (b[3] - b[2]) / (ny - 1)
+    dz = (b[5] - b[4]) / (nzz - 1) if nzz > 1 else 0.0
+    w = ny if face <= 1 else nx
+    h = nzz if face <= 3 else ny
+    for q in range(h):
+        for a in range(w):
+            if face <= 1:
+                yield (b[0] if face == 0 else b[1]), b[2] + a * dy, (b[4] + q * dz if nzz > 1 else 0.0)
+            elif face <= 3:
+                yield b[0] + a * dx, (b[2] if face == 2 else b[3]), (b[4] + q * dz if nzz > 1 else 0.0)
+            else:
+                yield b[0] + a * dx, b[2] + q * dy, (b[4] if face == 4 else b[5])
+
+
+def _eval_bc(latex, lin, x, y, z):
+    """EvalExpr (src/backends/cpu/cpu_utils.cpp:520-530) over the host evaluation."""
+    if latex:
+        try:
+            v = solver.expression_value(latex, x, y, z)
+            if np.isfinite(v):
+                return v
+        except solver.SolveError:
+            pass
+    return lin[0] + lin[1] * x + lin[2] * y + lin[3] * z
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nz", [1, 9])
+def test_gpu_face_expressions_with_linear_fallback(lib, nz):
+    b = (-1.0, 2.0, 0.5, 1.5, -0.25, 0.75)
+    g = _grid(17, 11, nz, b)
+    lin = (0.5, -1.25, 2.0, 0.75)
+    forms = [r"\sin(\pi*x)\cos(y) + z", r"\frac{1}{x}", r"\log(y - 1)", r"\sin(\pi x)", "", None]
+    for face in range(6 if nz > 1 else 4):
+        for latex in forms:
+            got = solver.eval_face_expression(latex, g, face, lin)
+            ref = np.array([_eval_bc(latex, lin, x, y, z) for x, y, z in _face_nodes(face, 17, 11, nz, b)])
+            _same(got, ref, rtol=1e-13, afloor=1e-14)
