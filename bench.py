@@ -219,6 +219,83 @@ def bench_batched(lib, abi, n2d=2048, n3d=256, reps=3):
             "speedup_vs_plain_fp64": batched_rate / plain_rate}
 
 
+def bench_output(field, n, reps=3):
+    """Output and input forms around the solve, on the headline grid: the
+    legacy ASCII VTK and the VTI (with the CLI's derived fields) files of the
+    solution, formatted on the GPU and written to a tmpfs file (so the file
+    system does not bound the number), and a LaTeX right side evaluated at
+    every node on the GPU. The reference's CPU writers and per-node evaluator
+    are timed on a 16-plane sample and scaled to the grid."""
+    import tempfile
+
+    import torch
+
+    from pde_solver_b200 import solver
+    from pde_solver_b200.problem import GridProblem
+
+    p = GridProblem(n, n, n, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), a=-1.0, b=-1.0, az=-1.0)
+    tmp = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    out = {"grid": f"{n}^3", "file_system": "tmpfs" if tmp.startswith("/dev/shm") else "default temp dir"}
+    try:
+        for kind, fn in (("vtk_legacy", solver.write_vtk), ("vti_derived", solver.write_vti)):
+            path = os.path.join(tmp, "out." + kind)
+            fn(path, p, field.data_ptr())
+            ts = []
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                fn(path, p, field.data_ptr())
+                ts.append(time.perf_counter() - t0)
+            size = os.path.getsize(path)
+            out[kind] = {"ms": 1e3 * statistics.median(ts), "mb": size / 1e6,
+                         "file_gbs": size / statistics.median(ts) / 1e9}
+            os.remove(path)
+        latex = r"-3\pi^2\sin(\pi*x)\sin(\pi*y)\sin(\pi*z) + \exp(-(x^2+y^2+z^2))"
+        dev = torch.empty(p.n, dtype=torch.float64, device=field.device)
+        solver.eval_expression(latex, p, out=dev.data_ptr())
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            solver.eval_expression(latex, p, out=dev.data_ptr())
+            ts.append(time.perf_counter() - t0)
+        out["expression"] = {"latex": latex, "ms": 1e3 * statistics.median(ts),
+                             "nodes_per_s": p.n / statistics.median(ts)}
+        if oracle_available():
+            from oracle import oracle
+
+            ps = GridProblem(n, n, 16, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), a=-1.0, b=-1.0, az=-1.0)
+            fs = field[: ps.n].cpu().numpy()
+            scale = n / 16.0
+            t0 = time.perf_counter()
+            oracle.ref_write_vtk(os.path.join(tmp, "r.vtk"), ps, fs)
+            out["vtk_legacy"]["reference_cpu_ms"] = 1e3 * (time.perf_counter() - t0) * scale
+            t0 = time.perf_counter()
+            oracle.ref_write_vti(os.path.join(tmp, "r.vti"), ps, fs)
+            out["vti_derived"]["reference_cpu_ms"] = 1e3 * (time.perf_counter() - t0) * scale
+            t0 = time.perf_counter()
+            oracle.ref_materialize(latex, ps)
+            out["expression"]["reference_cpu_ms"] = 1e3 * (time.perf_counter() - t0) * scale
+            out["reference_sample"] = (f"reference writers / ExpressionEvaluator (oracle/_ref) on {n}x{n}x16, "
+                                       f"one host thread, scaled by {scale:.2f}")
+            for k in ("vtk_legacy", "vti_derived", "expression"):
+                out[k]["speedup_vs_reference_cpu"] = out[k]["reference_cpu_ms"] / out[k]["ms"]
+    finally:
+        for f in os.listdir(tmp):
+            os.remove(os.path.join(tmp, f))
+        os.rmdir(tmp)
+    return out
+
+
+def oracle_available():
+    try:
+        from oracle import oracle
+
+        return oracle.have_reference()
+    except Exception:
+        return False
+
+
 def bench_serving(abi, count=256, seed=7):
     """Serving form: a stream of Poisson requests (2D sides 65..513, 3D sides
     65..129, k log-normal sigma=0.5) submitted at once (saturation) to a
@@ -470,7 +547,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_forms:
         try:
-            line["forms"] = {"batched": bench_batched(lib, abi), "serving": bench_serving(abi)}
+            line["forms"] = {"batched": bench_batched(lib, abi), "serving": bench_serving(abi),
+                             "output": bench_output(out_dev, n)}
         except Exception as exc:  # the forms never block the headline line
             line["forms"] = {"error": str(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

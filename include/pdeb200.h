@@ -359,6 +359,45 @@ pdeb200_status pdeb200_expression_value(const char* latex, double x, double y, d
                                         double t, double* value, char* message,
                                         size_t message_len);
 
+/* ---- VTK output of a grid field ----------------------------------------- */
+
+/* Called as the write advances; fraction in [0, 1]. */
+typedef void (*pdeb200_write_progress)(double fraction, void* user);
+
+/* Legacy ASCII STRUCTURED_POINTS file, byte-identical to the reference's
+ * WriteVtkStructuredPoints (src/vtk_writer.cpp:28-82): the header with the
+ * ostream's default number format, then every value cast to float and printed
+ * fixed with 6 decimals, followed by a space, with a newline after each x row.
+ * The text is formatted on the GPU and written in chunks that overlap the
+ * formatting of the next chunk. Only the geometry of `grid` is used (nz <= 1
+ * writes nz = 1; the z bounds appear in ORIGIN and SPACING as given).
+ * `field` holds nx*ny*nz doubles, a device pointer when mem_space is
+ * PDEB200_MEM_DEVICE. Errors: PDEB200_ERR_INVALID with the reference's
+ * "invalid grid dimensions" / "failed to open output file". */
+pdeb200_status pdeb200_write_vtk(const char* path, const pdeb200_problem* grid, const double* field,
+                                 int32_t mem_space, int32_t device, pdeb200_write_progress progress,
+                                 void* user, char* message, size_t message_len);
+
+/* XML ImageData file (.vti) with base64 Float32 arrays, byte-identical to
+ * WriteVtkXmlImageData (src/vtk_writer.cpp:176-268). With `derived` set it
+ * adds the derived fields of ComputeDerivedFields (src/vtk_writer.cpp:365-440)
+ * in the order BuildDerivedFieldVectors lists them (src/main.cpp:255-288):
+ * gradient_x, gradient_y, [gradient_z], laplacian, flux_x, flux_y, [flux_z],
+ * energy_norm, with the flux coefficients grid->a, grid->b, grid->az. Each
+ * array is computed and encoded on the GPU in one pass over the field. */
+pdeb200_status pdeb200_write_vti(const char* path, const pdeb200_problem* grid, const double* field,
+                                 int32_t derived, int32_t mem_space, int32_t device,
+                                 pdeb200_write_progress progress, void* user, char* message,
+                                 size_t message_len);
+
+/* The value text of the legacy file (everything after LOOKUP_TABLE) made on
+ * the host by the same formatter the GPU runs, for checking the formatter
+ * without a GPU; the writers never call it. Writes at most `capacity` bytes
+ * and sets *length to the full text length (PDEB200_ERR_INVALID when it did
+ * not fit). out may be NULL to ask for the length. */
+pdeb200_status pdeb200_vtk_values_host(const double* field, int64_t n, int32_t nx, char* out,
+                                       size_t capacity, size_t* length);
+
 #ifdef __cplusplus
 }
 #endif

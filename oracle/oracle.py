@@ -93,6 +93,10 @@ def reference() -> C.CDLL:
         lib.pderef_project.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.c_double, DP, DP, DP, DP, C.c_int, C.c_double, C.c_int, DP]
         lib.pderef_self_test.restype = C.c_int
+        lib.pderef_write_vtk.restype = C.c_int
+        lib.pderef_write_vtk.argtypes = [C.c_char_p, P(abi.Problem), DP, C.c_char_p, C.c_size_t]
+        lib.pderef_write_vti.restype = C.c_int
+        lib.pderef_write_vti.argtypes = [C.c_char_p, P(abi.Problem), DP, C.c_int, C.c_char_p, C.c_size_t]
         lib.pderef_set_threads.argtypes = [C.c_int]
         lib.pderef_max_threads.restype = C.c_int
         _ref = lib
@@ -207,6 +211,24 @@ def ref_materialize(latex, prob, t=0.0):
     if st != 0:
         raise RuntimeError(err.value.decode())
     return out
+
+
+def ref_write_vtk(path, prob, grid):
+    """WriteVtkStructuredPoints (src/vtk_writer.cpp:28-82) of `grid` on prob's geometry."""
+    grid = np.ascontiguousarray(grid, dtype=np.float64)
+    err = C.create_string_buffer(256)
+    cp = prob.to_c()
+    if reference().pderef_write_vtk(str(path).encode(), C.byref(cp), _dp(grid), err, 256) != 0:
+        raise RuntimeError(err.value.decode())
+
+
+def ref_write_vti(path, prob, grid, derived=True):
+    """WriteVtkXmlImageData (src/vtk_writer.cpp:176-268) with the CLI's derived fields."""
+    grid = np.ascontiguousarray(grid, dtype=np.float64)
+    err = C.create_string_buffer(256)
+    cp = prob.to_c()
+    if reference().pderef_write_vti(str(path).encode(), C.byref(cp), _dp(grid), 1 if derived else 0, err, 256) != 0:
+        raise RuntimeError(err.value.decode())
 
 
 def ref_project(u, v, w, p, nx, ny, nz, dx, dy, dz, dt, max_iter=1000, tol=1e-8, fix_corner=1):

@@ -11,6 +11,7 @@
 //   ProjectVelocity2D / ProjectVelocity3D          src/pressure_projection.cpp:255,698
 //   ComputeResidualNorms                           src/residual.cpp:153
 //   RunSelfTest                                    src/self_test.cpp:224
+//   WriteVtkStructuredPoints / WriteVtkXmlImageData src/vtk_writer.cpp:28,176
 // Built with PDEREF_DROPIN (oracle/_ref/libdropin.so) it also drives the
 // reference's SolveWithBackend with the CUDA backend compiled in and served by
 // the B200 shim (pde_solver_b200/shim/cuda_solver_shim.cpp).
@@ -28,6 +29,7 @@
 #include "residual.h"
 #include "self_test.h"
 #include "solver.h"
+#include "vtk_io.h"
 #ifdef PDEREF_DROPIN
 #include "cuda_solver.h"
 SolveOutput SolvePDETimeSeriesCuda(const SolveInput& input, const FrameCallback& on_frame,
@@ -296,6 +298,71 @@ int pderef_project(int nx, int ny, int nz, double dx, double dy, double dz, doub
 // The reference's own analytic self-test (src/self_test.cpp:224-411); returns
 // 1 when any case fails.
 int pderef_self_test(void) { return RunSelfTest(); }
+
+// The reference's VTK writers on a Domain built from the problem's geometry
+// (nz <= 1 gives Domain::nz = 1). derived != 0 passes the derived fields the
+// way the reference CLI does (BuildDerivedFieldVectors, src/main.cpp:255-288).
+Domain DomainOf(const pdeb200_problem* p) {
+  Domain d;
+  d.nx = p->nx;
+  d.ny = p->ny;
+  d.nz = p->nz <= 1 ? 1 : p->nz;
+  d.xmin = p->xmin;
+  d.xmax = p->xmax;
+  d.ymin = p->ymin;
+  d.ymax = p->ymax;
+  d.zmin = p->zmin;
+  d.zmax = p->zmax;
+  return d;
+}
+
+int pderef_write_vtk(const char* path, const pdeb200_problem* p, const double* grid, char* err, size_t err_len) {
+  const Domain d = DomainOf(p);
+  const std::vector<double> g(grid, grid + static_cast<size_t>(d.nx) * d.ny * d.nz);
+  VtkWriteResult r = WriteVtkStructuredPoints(path, d, g);
+  if (!r.ok) {
+    CopyError(r.error, err, err_len);
+    return 1;
+  }
+  return 0;
+}
+
+int pderef_write_vti(const char* path, const pdeb200_problem* p, const double* grid, int derived, char* err,
+                     size_t err_len) {
+  const Domain d = DomainOf(p);
+  const std::vector<double> g(grid, grid + static_cast<size_t>(d.nx) * d.ny * d.nz);
+  std::vector<std::vector<double>> data;
+  std::vector<std::string> names;
+  if (derived) {
+    DerivedFields f = ComputeDerivedFields(d, g, p->a, p->b, p->az);
+    data.push_back(f.gradient_x);
+    names.push_back("gradient_x");
+    data.push_back(f.gradient_y);
+    names.push_back("gradient_y");
+    if (d.nz > 1) {
+      data.push_back(f.gradient_z);
+      names.push_back("gradient_z");
+    }
+    data.push_back(f.laplacian);
+    names.push_back("laplacian");
+    data.push_back(f.flux_x);
+    names.push_back("flux_x");
+    data.push_back(f.flux_y);
+    names.push_back("flux_y");
+    if (d.nz > 1) {
+      data.push_back(f.flux_z);
+      names.push_back("flux_z");
+    }
+    data.push_back(f.energy_norm);
+    names.push_back("energy_norm");
+  }
+  VtkWriteResult r = WriteVtkXmlImageData(path, d, g, derived ? &data : nullptr, derived ? &names : nullptr);
+  if (!r.ok) {
+    CopyError(r.error, err, err_len);
+    return 1;
+  }
+  return 0;
+}
 
 #ifdef PDEREF_DROPIN
 // Drop-in harness: the same SolveInput through the reference's dispatch with

@@ -285,6 +285,7 @@ class ServerStats(C.Structure):
     ]
 
 
+WRITE_PROGRESS = C.CFUNCTYPE(None, C.c_double, C.c_void_p)
 FRAME_CB = C.CFUNCTYPE(C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -333,6 +334,15 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.pdeb200_eval_face_expression.restype = C.c_int32
     lib.pdeb200_eval_face_expression.argtypes = [C.c_char_p, P(C.c_double), P(Problem), C.c_int32, C.c_double,
                                                  C.c_int32, C.c_void_p, C.c_int32, C.c_char_p, C.c_size_t]
+    lib.pdeb200_write_vtk.restype = C.c_int32
+    lib.pdeb200_write_vtk.argtypes = [C.c_char_p, P(Problem), C.c_void_p, C.c_int32, C.c_int32, WRITE_PROGRESS,
+                                      C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.pdeb200_write_vti.restype = C.c_int32
+    lib.pdeb200_write_vti.argtypes = [C.c_char_p, P(Problem), C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                      WRITE_PROGRESS, C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.pdeb200_vtk_values_host.restype = C.c_int32
+    lib.pdeb200_vtk_values_host.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.c_char_p, C.c_size_t,
+                                            P(C.c_size_t)]
     lib.pdeb200_expression_value.restype = C.c_int32
     lib.pdeb200_expression_value.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double,
                                              P(C.c_double), C.c_char_p, C.c_size_t]

@@ -113,6 +113,7 @@ struct Context {
   std::string name;
   std::mutex mu;
   long long launches = 0;
+  std::shared_ptr<void> io_staging;  // output staging buffers, kept between writes (vtk.cu)
 
   cudaEvent_t ev_get() {
     if (!evpool.empty()) {

@@ -64,6 +64,7 @@ void init_context(Context* c, int dev) {
 void free_context(Context* c) {
   cudaSetDevice(c->dev);
   cudaStreamSynchronize(c->stream);
+  c->io_staging.reset();
   cudaFree(c->d_ctl);
   cudaFreeHost(c->h_ctl);
   cudaFree(c->d_partials);

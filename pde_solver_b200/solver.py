@@ -111,6 +111,47 @@ def eval_face_expression(latex: str | None, problem: GridProblem, face: int, lin
     return res
 
 
+def _write(fn, path, problem, field, extra, device, progress):
+    lib = _lib()
+    cp = problem.to_c()
+    msg = C.create_string_buffer(256)
+    cb = abi.WRITE_PROGRESS(lambda f, u: progress(f)) if progress else abi.WRITE_PROGRESS()
+    if isinstance(field, np.ndarray):
+        field = np.ascontiguousarray(field, dtype=np.float64)
+        ptr, mem = field.ctypes.data_as(C.c_void_p), abi.MEM_HOST
+    else:
+        ptr, mem = C.c_void_p(field), abi.MEM_DEVICE
+    st = getattr(lib, fn)(str(path).encode(), C.byref(cp), ptr, *extra, mem, device, cb, None, msg, 256)
+    if st != abi.OK:
+        raise SolveError(st, msg.value.decode() or lib.pdeb200_status_string(st).decode())
+
+
+def write_vtk(path, problem: GridProblem, field, device: int = 0, progress=None):
+    """Legacy ASCII VTK file of `field` (host array, or device pointer as int),
+    byte-identical to WriteVtkStructuredPoints (src/vtk_writer.cpp:28-82);
+    formatted on the GPU."""
+    _write("pdeb200_write_vtk", path, problem, field, (), device, progress)
+
+
+def write_vti(path, problem: GridProblem, field, derived: bool = True, device: int = 0, progress=None):
+    """VTK XML ImageData file (base64 Float32), byte-identical to
+    WriteVtkXmlImageData (src/vtk_writer.cpp:176-268) with the derived fields
+    the reference CLI adds (flux coefficients problem.a, problem.b, problem.az)."""
+    _write("pdeb200_write_vti", path, problem, field, (1 if derived else 0,), device, progress)
+
+
+def vtk_values_host(field, nx: int) -> bytes:
+    """The legacy file's value text from the host copy of the GPU formatter."""
+    lib = _lib()
+    field = np.ascontiguousarray(field, dtype=np.float64)
+    n = C.c_size_t()
+    assert lib.pdeb200_vtk_values_host(field.ctypes.data_as(C.c_void_p), field.size, nx, None, 0, C.byref(n)) == 0
+    buf = C.create_string_buffer(n.value)
+    st = lib.pdeb200_vtk_values_host(field.ctypes.data_as(C.c_void_p), field.size, nx, buf, n.value, C.byref(n))
+    assert st == abi.OK
+    return buf.raw[:n.value]
+
+
 def expression_value(latex: str, x: float, y: float, z: float = 0.0, t: float = 0.0) -> float:
     """One host evaluation of the compiled expression (no GPU needed)."""
     lib = _lib()

@@ -141,3 +141,27 @@ def expression_errors():
         r"\atan2{y, x}",
         r"\operatorname{atan2}{y, x}",
     ]
+
+
+def vtk_cases():
+    """Fields for the VTK writers: (name, problem geometry, field). Values mix
+    smooth data with the formatter's edge cases: exact decimal ties, negative
+    zero, tiny negatives, subnormals, huge values, +-inf and NaN of both signs."""
+    rng = np.random.default_rng(2024)
+    special = np.array([0.0078125, -0.0078125, 2.0**-20, 0.5, 2.5, -0.0, -1e-9, 1e-45, 3.4e38, -3.4e38,
+                        0.9999995, 123456.7890625, 1e300, -1e300, np.inf, -np.inf, np.nan,
+                        -np.nan, 4.0e9, 16777217.0, 1.0 / 3.0, 2.0 / 3.0], dtype=np.float64)
+    special[17] = np.copysign(np.nan, -1.0)
+    out = []
+    p = GridProblem(9, 7, 1, bounds=(-1.0, 1.0, 0.0, 3.0, 0.0, 1.0), a=-1.0, b=-2.0, az=-0.5)
+    f = np.sin(np.linspace(0.0, 7.0, p.n)) * 10.0 ** rng.integers(-8, 6, p.n)
+    f[:special.size] = special
+    out.append(("field_2d", p, f))
+    p = GridProblem(6, 5, 4, bounds=(0.0, 1.0, -0.5, 0.5, 0.25, 2.0), a=-1.0, b=-1.0, az=-3.0)
+    x, y, z = p.coords()
+    out.append(("smooth_3d", p, np.exp(-x) * np.cos(3.0 * y) + z * z))
+    p = GridProblem(3, 3, 1, bounds=(0.0, 1e-3, 0.0, 2.5e6, 0.0, 0.0))
+    out.append(("tiny_2d", p, rng.standard_normal(p.n)))
+    p = GridProblem(1, 2, 1, bounds=(0.0, 0.0, 0.0, 1.0, 0.0, 1.0))
+    out.append(("single_column", p, np.array([1.25, -7.5])))
+    return out
