@@ -602,6 +602,7 @@ __device__ __noinline__ void bcoarse_solve(const BLevel& C, int sweeps) {
     }
   }
   __syncthreads();
+  if (total == 1 && sweeps > 1) sweeps = 1;  // one interior node: the first sweep is the fixed point
   for (int s = 0; s < sweeps; ++s)
     for (int color = 0; color < 2; ++color) {
       for (int t = threadIdx.x; t < total; t += blockDim.x) {

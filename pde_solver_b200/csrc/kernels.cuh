@@ -72,6 +72,9 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, c
     long long id = ((long long)k0 * g.ny + j) * g.nx + i;
     T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
     T zc = x[id];
+    // two planes per trip: the loads of the second are issued before the
+    // first plane's result is stored (more bytes in flight per thread)
+#pragma unroll 2
     for (int k = k0; k < k1; ++k, id += g.sxy) {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       Stencil<T> s = cf.template at<T>(g, id);
@@ -102,6 +105,7 @@ __global__ void __launch_bounds__(kBx* kBy) k_residual_folded(GridDev g, Coef cf
     long long id = ((long long)k0 * g.ny + j) * g.nx + i;
     T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
     T zc = x[id];
+#pragma unroll 2
     for (int k = k0; k < k1; ++k, id += g.sxy) {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       Stencil<T> s = cf.template at<T>(g, id);
@@ -1026,6 +1030,7 @@ __global__ void k_coarse_solve_smem(GridDev g, Coef cf, const TB* __restrict__ b
   }
   __syncthreads();
   const int sxy = (int)g.sxy, nx = g.nx;
+  if (total == 1) sweeps = sweeps < 1 ? sweeps : 1;  // one interior node: the first sweep is the fixed point
   for (int s = 0; s < sweeps; ++s)
     for (int color = 0; color < 2; ++color) {
       for (int t = tid; t < total; t += blockDim.x) {
@@ -1165,11 +1170,16 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
       __syncthreads();
     }
   }
-  // coarsest level: sweeps from zero
+  // coarsest level: sweeps from zero. With a single interior node (3 nodes a
+  // side) the first sweep is already the fixed point (its neighbours are
+  // boundary zeros), so the remaining sweeps, which would rewrite the same
+  // value, are skipped.
   {
     const TailLevel<Coef, T>& L = lv[nlev - 1];
+    const GridDev& g = L.g;
+    const int total = (g.nx - 2) * (g.ny - 2) * (g.dim == 3 ? g.nz - 2 : 1);
     tail_zero(L);
-    tail_sweeps(L, nlev == 1 ? rhs0 : L.b, coarse_iters, 0);
+    tail_sweeps(L, nlev == 1 ? rhs0 : L.b, total == 1 ? 1 : coarse_iters, 0);
   }
   // up: prolong-add, post-smooth
   for (int l = nlev - 2; l >= 0; --l) {
