@@ -151,6 +151,24 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
   column_range(g, k0, k1);
   if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) return;
   int k = k0 + ((i + j + k0 + color) & 1);
+  // nodes k and k+2 of one colour per trip: neither reads the other (their
+  // neighbours are all of the other colour), so both nodes' loads are issued
+  // before either store
+  for (; k + 2 < k1; k += 4) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i, id2 = id + 2 * g.sxy;
+    Stencil<T> s = cf.template at<T>(g, id);
+    Stencil<T> s2 = cf.template at<T>(g, id2);
+    const T b1 = T(b[id]), b2 = T(b[id2]);
+    const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+    const T mid = g.dim == 3 ? x[id + g.sxy] : T(0);  // zp of node k, zm of node k+2
+    const T zp2 = g.dim == 3 ? x[id2 + g.sxy] : T(0);
+    const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
+    const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
+    fold_faces<T>(g, i, j, k, s, nullptr);
+    fold_faces<T>(g, i, j, k + 2, s2, nullptr);
+    x[id] = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, g.dim)) / s.c;
+    x[id2] = (b2 - nb_sum<T>(s2, xp2, xm2, yp2, ym2, zp2, mid, g.dim)) / s2.c;
+  }
   for (; k < k1; k += 2) {
     const long long id = ((long long)k * g.ny + j) * g.nx + i;
     Stencil<T> s = cf.template at<T>(g, id);
@@ -880,6 +898,7 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict_march(GridDev gf, GridDev
   }
   // nested 2:1 in z: coarse K takes fine planes 2K-1, 2K, 2K+1 with 1/4, 1/2, 1/4
   double below = 2 * K0 - 1 >= 0 ? plane(2 * K0 - 1) : 0.0;
+#pragma unroll 2
   for (int K = K0; K < K1; ++K) {
     const double mid = plane(2 * K);
     const double above = 2 * K + 1 <= gf.nz - 1 ? plane(2 * K + 1) : 0.0;
@@ -935,15 +954,26 @@ __global__ void __launch_bounds__(kBx* kBy) k_prolong_march(GridDev gf, GridDev 
     vb = v;
     return v;
   };
-  for (int k = k0; k < k1; ++k) {
-    int K0 = 0;
-    double tz = 0.0;
-    if (gf.dim == 3) coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
-    const double y0 = at(K0);
-    const double y1 = tz != 0.0 ? at(K0 + 1) : y0;
-    const double v = (1.0 - tz) * y0 + tz * y1;
-    const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
-    xf[id] = T(double(xf[id]) + v);
+  // groups of four planes: the four fine values are loaded before any is
+  // stored, so a thread has four loads in flight instead of one
+  constexpr int kGroup = 4;
+  for (int kg = k0; kg < k1; kg += kGroup) {
+    T old[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q)
+      if (kg + q < k1) old[q] = xf[((long long)(kg + q) * gf.ny + j) * gf.nx + i];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const int k = kg + q;
+      if (k >= k1) break;
+      int K0 = 0;
+      double tz = 0.0;
+      if (gf.dim == 3) coarse_pos(k, gf.nz, gc.nz, zmode, K0, tz);
+      const double y0 = at(K0);
+      const double y1 = tz != 0.0 ? at(K0 + 1) : y0;
+      const double v = (1.0 - tz) * y0 + tz * y1;
+      xf[((long long)k * gf.ny + j) * gf.nx + i] = T(double(old[q]) + v);
+    }
   }
 }
 
