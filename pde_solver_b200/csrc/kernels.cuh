@@ -72,10 +72,12 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, c
     long long id = ((long long)k0 * g.ny + j) * g.nx + i;
     T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
     T zc = x[id];
+    int k = k0;
     // two planes per trip: the loads of the second are issued before the
-    // first plane's result is stored (more bytes in flight per thread)
+    // first plane's result is stored (more bytes in flight per thread). A
+    // hand-batched form like k_residual_folded's was slower here.
 #pragma unroll 2
-    for (int k = k0; k < k1; ++k, id += g.sxy) {
+    for (; k < k1; ++k, id += g.sxy) {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       Stencil<T> s = cf.template at<T>(g, id);
       fold_faces<T>(g, i, j, k, s, nullptr);
@@ -105,8 +107,31 @@ __global__ void __launch_bounds__(kBx* kBy) k_residual_folded(GridDev g, Coef cf
     long long id = ((long long)k0 * g.ny + j) * g.nx + i;
     T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
     T zc = x[id];
-#pragma unroll 2
-    for (int k = k0; k < k1; ++k, id += g.sxy) {
+    int k = k0;
+    // two planes per trip, all loads before the stores (see k_apply_folded)
+    for (; k + 1 < k1; k += 2, id += 2 * g.sxy) {
+      const long long id2 = id + g.sxy;
+      const T z1 = x[id2];
+      const T z2 = x[id2 + g.sxy];
+      const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
+      const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
+      const T b1 = T(b[id]), b2 = T(b[id2]);
+      Stencil<T> s = cf.template at<T>(g, id);
+      Stencil<T> s2 = cf.template at<T>(g, id2);
+      fold_faces<T>(g, i, j, k, s, nullptr);
+      fold_faces<T>(g, i, j, k + 1, s2, nullptr);
+      const T v = b1 - (s.c * zc + nb_sum<T>(s, xp1, xm1, yp1, ym1, z1, zm, g.dim));
+      const T v2 = b2 - (s2.c * z1 + nb_sum<T>(s2, xp2, xm2, yp2, ym2, z2, zc, g.dim));
+      r[id] = v;
+      r[id2] = v2;
+      if constexpr (NV > 0) {
+        acc[0] += double(v) * double(v);
+        acc[0] += double(v2) * double(v2);
+      }
+      zm = z1;
+      zc = z2;
+    }
+    for (; k < k1; ++k, id += g.sxy) {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       Stencil<T> s = cf.template at<T>(g, id);
       fold_faces<T>(g, i, j, k, s, nullptr);
@@ -863,6 +888,23 @@ struct FwColumn {
     restrict_weights(I, gf.nx, gc.nx, map_mode(gf.nx, gc.nx), ix0, wx);
     restrict_weights(J, gf.ny, gc.ny, map_mode(gf.ny, gc.ny), iy0, wy);
   }
+  // Interior column of a nested 2:1 map in x and y: taps (1/4, 1/2, 1/4) at
+  // 2I-1..2I+1 and 2J-1..2J+1, all in range. Same operations in the same
+  // order as plane(), without the weight tests, so all nine loads can be
+  // issued together.
+  __device__ __forceinline__ double plane_nested(int kf) const {
+    double acc = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const T* row = rf + ((long long)kf * ny + (iy0 + b)) * nx + ix0;
+      double rs = 0.0;
+      rs += 0.25 * double(row[0]);
+      rs += 0.5 * double(row[1]);
+      rs += 0.25 * double(row[2]);
+      acc += (b == 1 ? 0.5 : 0.25) * rs;
+    }
+    return acc;
+  }
   __device__ __forceinline__ double plane(int kf) const {
     double acc = 0.0;
 #pragma unroll
@@ -890,7 +932,9 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict_march(GridDev gf, GridDev
   const int K0 = blockIdx.z * chunk, K1 = min(gc.nz, K0 + chunk);
   FwColumn<T> col;
   col.init(gf, gc, rf, I, J);
-  auto plane = [&](int kf) -> double { return col.plane(kf); };
+  const bool nested = map_mode(gf.nx, gc.nx) == 1 && map_mode(gf.ny, gc.ny) == 1 && I >= 1 && I <= gc.nx - 2 &&
+                      J >= 1 && J <= gc.ny - 2;
+  auto plane = [&](int kf) -> double { return nested ? col.plane_nested(kf) : col.plane(kf); };
   const long long cxy = (long long)J * gc.nx + I;
   if (gc.dim != 3 || gc.nz == gf.nz) {
     for (int K = K0; K < K1; ++K) bc[(long long)K * gc.sxy + cxy] = TC(plane(K));
