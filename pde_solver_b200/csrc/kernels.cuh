@@ -166,7 +166,12 @@ __global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, con
 // One red-black Gauss-Seidel colour pass on the folded operator; colour of
 // (i,j,k) is (i+j+k)&1. The updated colour only reads the other colour, so a
 // pass is race free.
-template <class Coef, typename T, typename TB>
+// ZERO: the first pass of a sweep from a zero field. Every neighbour value
+// is zero, so none is loaded (the arithmetic is that of a pass over a
+// zero-filled field, so the bits are the same), and the field need not be
+// cleared first: the other colour is written by the next pass before any
+// pass reads it, and boundary entries are never written.
+template <class Coef, typename T, typename TB, bool ZERO = false>
 __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x,
                                                    int color, const Ctl* ctl) {
   if (ctl_skip(ctl)) return;
@@ -184,11 +189,15 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
     Stencil<T> s = cf.template at<T>(g, id);
     Stencil<T> s2 = cf.template at<T>(g, id2);
     const T b1 = T(b[id]), b2 = T(b[id2]);
-    const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-    const T mid = g.dim == 3 ? x[id + g.sxy] : T(0);  // zp of node k, zm of node k+2
-    const T zp2 = g.dim == 3 ? x[id2 + g.sxy] : T(0);
-    const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
-    const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
+    auto ld = [&](long long q) -> T {
+      if constexpr (ZERO) return T(0);
+      return x[q];
+    };
+    const T zm = g.dim == 3 ? ld(id - g.sxy) : T(0);
+    const T mid = g.dim == 3 ? ld(id + g.sxy) : T(0);  // zp of node k, zm of node k+2
+    const T zp2 = g.dim == 3 ? ld(id2 + g.sxy) : T(0);
+    const T xp1 = ld(id + 1), xm1 = ld(id - 1), yp1 = ld(id + g.nx), ym1 = ld(id - g.nx);
+    const T xp2 = ld(id2 + 1), xm2 = ld(id2 - 1), yp2 = ld(id2 + g.nx), ym2 = ld(id2 - g.nx);
     fold_faces<T>(g, i, j, k, s, nullptr);
     fold_faces<T>(g, i, j, k + 2, s2, nullptr);
     x[id] = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, g.dim)) / s.c;
@@ -198,9 +207,14 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
     const long long id = ((long long)k * g.ny + j) * g.nx + i;
     Stencil<T> s = cf.template at<T>(g, id);
     fold_faces<T>(g, i, j, k, s, nullptr);
-    const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
-    const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-    x[id] = (T(b[id]) - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
+    if constexpr (ZERO) {
+      const T z0 = T(0);
+      x[id] = (T(b[id]) - nb_sum<T>(s, z0, z0, z0, z0, z0, z0, g.dim)) / s.c;
+    } else {
+      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
+      const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
+      x[id] = (T(b[id]) - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
+    }
   }
 }
 

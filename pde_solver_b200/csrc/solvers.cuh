@@ -589,14 +589,24 @@ struct Hierarchy {
       }
     }
     if (!fused) {
-      // in place: the buffer never changes; flips are bookkeeping only
+      // in place: the buffer never changes; flips are bookkeeping only. From
+      // zero, the first pass reads no field values (k_rbgs ZERO) and the
+      // field is not cleared; without sweeps it is cleared.
       if (from_zero) {
-        ProfScope ps(ctx, "zero_fill", lvl, dofs * sizeof(T));
-        vfill<T>(ctx, L.g.n, L.xa, T(0), ctl);
         cur = L.xa;
+        if (sweeps == 0) {
+          ProfScope ps(ctx, "zero_fill", lvl, dofs * sizeof(T));
+          vfill<T>(ctx, L.g.n, L.xa, T(0), ctl);
+        }
       }
       for (int s = 0; s < sweeps; ++s) {
         for (int half = 0; half < 2; ++half) {
+          if (from_zero && s == 0 && half == 0) {
+            // b and the written half of x: 8 B per DOF in FP64
+            ProfScope ps(ctx, "rbgs_zero_pass", lvl, dofs * sizeof(T));
+            k_rbgs<Coef, T, T, true><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first, ctl);
+            continue;
+          }
           ProfScope ps(ctx, "rbgs_color_pass", lvl, dofs * 2.0 * sizeof(T));
           k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first ^ half, ctl);
         }
