@@ -73,10 +73,28 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, c
     T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
     T zc = x[id];
     int k = k0;
-    // two planes per trip: the loads of the second are issued before the
-    // first plane's result is stored (more bytes in flight per thread). A
-    // hand-batched form like k_residual_folded's was slower here.
-#pragma unroll 2
+    // two planes per trip, all loads before the stores (see k_residual_folded)
+    for (; k + 1 < k1; k += 2, id += 2 * g.sxy) {
+      const long long id2 = id + g.sxy;
+      const T z1 = x[id2];
+      const T z2 = x[id2 + g.sxy];
+      const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
+      const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
+      Stencil<T> s = cf.template at<T>(g, id);
+      Stencil<T> s2 = cf.template at<T>(g, id2);
+      fold_faces<T>(g, i, j, k, s, nullptr);
+      fold_faces<T>(g, i, j, k + 1, s2, nullptr);
+      const T v = s.c * zc + nb_sum<T>(s, xp1, xm1, yp1, ym1, z1, zm, g.dim);
+      const T v2 = s2.c * z1 + nb_sum<T>(s2, xp2, xm2, yp2, ym2, z2, zc, g.dim);
+      y[id] = v;
+      y[id2] = v2;
+      if constexpr (NV > 0) {
+        acc[0] += double(zc) * double(v);
+        acc[0] += double(z1) * double(v2);
+      }
+      zm = z1;
+      zc = z2;
+    }
     for (; k < k1; ++k, id += g.sxy) {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       Stencil<T> s = cf.template at<T>(g, id);
