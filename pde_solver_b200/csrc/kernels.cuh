@@ -189,15 +189,24 @@ __global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, con
 // zero-filled field, so the bits are the same), and the field need not be
 // cleared first: the other colour is written by the next pass before any
 // pass reads it, and boundary entries are never written.
-template <class Coef, typename T, typename TB, bool ZERO = false>
+// DOT: the sum over the updated nodes of b * (new x) is reduced over the grid
+// and handed to `post` (the last two passes of a V-cycle's finest level give
+// r.z of preconditioned CG, since b is r there).
+template <class Coef, typename T, typename TB, bool ZERO = false, bool DOT = false, class Post = NoPost>
 __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x,
-                                                   int color, const Ctl* ctl) {
+                                                   int color, const Ctl* ctl, RedSlot slot = RedSlot{},
+                                                   Post post = Post{}) {
   if (ctl_skip(ctl)) return;
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
   int k0, k1;
   column_range(g, k0, k1);
-  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) return;
+  double acc[1] = {0.0};
+  // with DOT every thread reaches the block reduction at the end
+  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) {
+    if constexpr (!DOT) return;
+    k1 = k0;  // no nodes: both loops below are empty
+  }
   int k = k0 + ((i + j + k0 + color) & 1);
   // nodes k and k+2 of one colour per trip: neither reads the other (their
   // neighbours are all of the other colour), so both nodes' loads are issued
@@ -218,8 +227,14 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
     const T xp2 = ld(id2 + 1), xm2 = ld(id2 - 1), yp2 = ld(id2 + g.nx), ym2 = ld(id2 - g.nx);
     fold_faces<T>(g, i, j, k, s, nullptr);
     fold_faces<T>(g, i, j, k + 2, s2, nullptr);
-    x[id] = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, g.dim)) / s.c;
-    x[id2] = (b2 - nb_sum<T>(s2, xp2, xm2, yp2, ym2, zp2, mid, g.dim)) / s2.c;
+    const T v1 = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, g.dim)) / s.c;
+    const T v2 = (b2 - nb_sum<T>(s2, xp2, xm2, yp2, ym2, zp2, mid, g.dim)) / s2.c;
+    x[id] = v1;
+    x[id2] = v2;
+    if constexpr (DOT) {
+      acc[0] += double(b1) * double(v1);
+      acc[0] += double(b2) * double(v2);
+    }
   }
   for (; k < k1; k += 2) {
     const long long id = ((long long)k * g.ny + j) * g.nx + i;
@@ -231,9 +246,13 @@ __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB*
     } else {
       const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
       const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-      x[id] = (T(b[id]) - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
+      const T bv = T(b[id]);
+      const T v = (bv - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
+      x[id] = v;
+      if constexpr (DOT) acc[0] += double(bv) * double(v);
     }
   }
+  if constexpr (DOT) grid_reduce<1, false>(acc, slot, post);
 }
 
 // One full red-black Gauss-Seidel sweep in a single pass (colour `first`

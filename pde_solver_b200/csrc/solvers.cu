@@ -154,8 +154,9 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
                                                               ctx->d_ctl);
     }
     ctx->count(2);
-    H.vcycle(ctx, r, ctx->d_ctl);
-    {
+    // beta from r.z: summed by the preconditioner's last two colour passes
+    // when it can, else by a separate dot
+    if (!H.vcycle_dot(ctx, r, ctx->d_ctl, ctx->slot())) {
       ProfScope ps(ctx, "dot", 0, dofs * 16.0);
       k_dot<double, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{ctx->d_ctl}, ctx->d_ctl);
     }

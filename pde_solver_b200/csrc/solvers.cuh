@@ -92,6 +92,22 @@ struct PostRZ {
   __device__ void operator()(const double* v) const { c->rz = v[0]; }
 };
 
+// r.z summed by the last two colour passes of a V-cycle (k_rbgs DOT): the
+// first stores its colour's part, the second adds its own and forms beta
+constexpr int kAuxRzPart = 7;
+struct PostRZPart {
+  Ctl* c;
+  __device__ void operator()(const double* v) const { c->aux[kAuxRzPart] = v[0]; }
+};
+struct PostBetaSplit {
+  Ctl* c;
+  __device__ void operator()(const double* v) const {
+    const double rz = c->aux[kAuxRzPart] + v[0];
+    c->beta = rz / c->rz;
+    c->rz = rz;
+  }
+};
+
 // |b|^2 of the relative rule: tol2 = tol^2 |b|^2, immediate exit for b = 0
 struct PostBB {
   Ctl* c;
@@ -686,11 +702,44 @@ struct Hierarchy {
         k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
     }
     ctx->count();
-    cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l);
+    if (l == 0 && dot_slot && post > 0 && !fused && !L.single_pass) {
+      // the last sweep's two passes also sum r.z (b is r on level 0)
+      cur = sweeps_from(ctx, L, b, cur, post - 1, 1, false, ctl, l);
+      const dim3 grid = stencil_grid_auto(L.g), block = stencil_block();
+      {
+        ProfScope ps(ctx, "rbgs_color_pass", l, dofs * 2.0 * sizeof(T));
+        k_rbgs<Coef, T, T, false, true, PostRZPart><<<grid, block, 0, ctx->stream>>>(
+            L.g, L.cf, b, cur, 1, ctl, *dot_slot, PostRZPart{const_cast<Ctl*>(ctl)});
+      }
+      {
+        ProfScope ps(ctx, "rbgs_color_pass", l, dofs * 2.0 * sizeof(T));
+        k_rbgs<Coef, T, T, false, true, PostBetaSplit><<<grid, block, 0, ctx->stream>>>(
+            L.g, L.cf, b, cur, 0, ctl, *dot_slot, PostBetaSplit{const_cast<Ctl*>(ctl)});
+      }
+      ctx->count(2);
+      dot_done = true;
+    } else {
+      cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l);
+    }
   }
 
   // z = M rhs0; the result is in levels[0].out
-  void vcycle(Context* ctx, const T* rhs0, const Ctl* ctl) { level(ctx, 0, rhs0, ctl); }
+  void vcycle(Context* ctx, const T* rhs0, const Ctl* ctl) {
+    dot_slot = nullptr;
+    level(ctx, 0, rhs0, ctl);
+  }
+  // z = M r and, when the finest level's last sweep could carry it, beta of
+  // preconditioned CG from r.z (PostBetaSplit). Returns false when the caller
+  // must compute r.z itself.
+  bool vcycle_dot(Context* ctx, const T* r, const Ctl* ctl, const RedSlot& slot) {
+    dot_slot = &slot;
+    dot_done = false;
+    level(ctx, 0, r, ctl);
+    dot_slot = nullptr;
+    return dot_done;
+  }
+  const RedSlot* dot_slot = nullptr;
+  bool dot_done = false;
   T* z() const { return levels[0].out; }
 };
 
