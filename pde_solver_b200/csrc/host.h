@@ -222,7 +222,11 @@ dim3 stencil_grid(const GridDev& g, int zchunk = 16);
 dim3 stencil_grid_full(const GridDev& g, int zchunk = 16);
 // z-chunking chosen for occupancy: about kTargetBlocks blocks, at least one
 // interior plane per thread
-dim3 stencil_grid_auto(const GridDev& g);
+dim3 stencil_grid_auto(const GridDev& g, long long target_blocks = 0);
+// launch shape of the colour passes (k_rbgs): about three waves of the three
+// blocks per SM their registers allow, measured faster than the default
+// target on every level of the 257^3 hierarchy
+inline dim3 rbgs_grid(const GridDev& g) { return stencil_grid_auto(g, 148 * 9); }
 // launch shape of the fused red-black sweep (64 x 8 column tiles)
 dim3 fused_grid(const GridDev& g);
 // launch shape of the staged single-pass sweep (32 x 8 column tiles, z chunks

@@ -110,8 +110,8 @@ dim3 stencil_grid(const GridDev& g, int zchunk) {
   return dim3(xy.x, xy.y, cap_chunks((long long)xy.x * xy.y, chunks));
 }
 
-dim3 stencil_grid_auto(const GridDev& g) {
-  const long long kTargetBlocks = 148 * 16;
+dim3 stencil_grid_auto(const GridDev& g, long long target_blocks) {
+  const long long kTargetBlocks = target_blocks > 0 ? target_blocks : 148 * 16;
   const int kint = g.dim == 3 ? g.nz - 2 : 1;
   const dim3 xy((g.nx + kBx - 1) / kBx, (g.ny + kBy - 1) / kBy, 1);
   const long long xyb = (long long)xy.x * xy.y;

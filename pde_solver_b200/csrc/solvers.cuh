@@ -575,7 +575,8 @@ struct Hierarchy {
   bool fused = false;
   T* sweeps_from(Context* ctx, Level& L, const T* b, T* cur, int sweeps, int first, bool from_zero,
                  const Ctl* ctl, int lvl) {
-    const dim3 grid = stencil_grid_auto(L.g), block = stencil_block();
+    const dim3 grid = rbgs_grid(L.g), block = stencil_block();
+    const dim3 zgrid = stencil_grid_auto(L.g);  // the pass from zero (fewer registers) keeps the default
     const double dofs = interior_dofs(L.g);
     if constexpr (kSweepCoef) {
       if (L.single_pass) {
@@ -620,7 +621,7 @@ struct Hierarchy {
           if (from_zero && s == 0 && half == 0) {
             // b and the written half of x: 8 B per DOF in FP64
             ProfScope ps(ctx, "rbgs_zero_pass", lvl, dofs * sizeof(T));
-            k_rbgs<Coef, T, T, true><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first, ctl);
+            k_rbgs<Coef, T, T, true><<<zgrid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first, ctl);
             continue;
           }
           ProfScope ps(ctx, "rbgs_color_pass", lvl, dofs * 2.0 * sizeof(T));
@@ -705,7 +706,7 @@ struct Hierarchy {
     if (l == 0 && dot_slot && post > 0 && !fused && !L.single_pass) {
       // the last sweep's two passes also sum r.z (b is r on level 0)
       cur = sweeps_from(ctx, L, b, cur, post - 1, 1, false, ctl, l);
-      const dim3 grid = stencil_grid_auto(L.g), block = stencil_block();
+      const dim3 grid = rbgs_grid(L.g), block = stencil_block();
       {
         ProfScope ps(ctx, "rbgs_color_pass", l, dofs * 2.0 * sizeof(T));
         k_rbgs<Coef, T, T, false, true, PostRZPart><<<grid, block, 0, ctx->stream>>>(
