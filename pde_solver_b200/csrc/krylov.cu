@@ -673,48 +673,60 @@ __global__ void k_add_scaled(long long n, double* __restrict__ x, const T* __res
   for (long long t = gtid(); t < n; t += gstride()) x[t] += s * double(e[t]);
 }
 
-// MG-PCG core in precision T (relative rule on the recursive residual)
+// MG-PCG core in precision T (relative rule on the recursive residual). One
+// object serves every outer step of a refinement: its vectors and the
+// captured iteration (the same b, x and hierarchy buffers each time) are made
+// once, so later steps neither allocate nor capture.
 template <class Coef, class HierT, typename T>
-pdeb200_status mg_pcg_core(Context* ctx, HierT& H, const GridDev& g, const Coef& cf, const T* b, T* x, int max_iter,
-                           double tol, const pdeb200_options* o, int* iters) {
-  const long long n = g.n;
-  Buf buf(sizeof(T) * n * 3, ctx->stream);
-  T* B = buf.template as<T>();
-  T *r = B, *p = B + n, *q = B + 2 * n;
-  PDEB_CUDA(cudaMemsetAsync(B, 0, sizeof(T) * n * 3, ctx->stream));
-  PDEB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, ctx->stream));
-  PDEB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-  ctl_init(ctx, max_iter, tol, 1e-300);
-  Ctl* C = ctx->d_ctl;
-  const int nb = vec_blocks(n, ctx);
-  k_dot<T, PostBB><<<nb, 256, 0, ctx->stream>>>(n, b, b, ctx->slot(), PostBB{C}, C);
-  T* z = H.z();
-  H.vcycle(ctx, r, C);
-  k_dot<T, PostRZ><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostRZ{C}, C);
-  k_cg_p<T><<<nb, 256, 0, ctx->stream>>>(n, p, z, C, 1);
-  ctx->count(3);
-  const dim3 grid = stencil_grid_auto(g), block = stencil_block();
-  auto iterate = [&](int) {
-    k_apply_folded<Coef, T, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(), PostAlpha{C}, C);
-    k_cg_xr<T, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, x, r, p, q, ctx->slot(), PostRRRel{C}, C);
-    H.vcycle(ctx, r, C);
-    k_dot<T, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{C}, C);
-    k_cg_p<T><<<nb, 256, 0, ctx->stream>>>(n, p, z, C, 0);
-    ctx->count(4);
-  };
+struct MgPcgCore {
+  Buf buf;
   IterGraph graph;
-  const bool graphed = graph.capture(ctx, iterate);
-  auto step = [&](int it) {
-    if (graphed)
-      graph.launch(ctx);
-    else
-      iterate(it);
-  };
-  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
-  const Ctl c = ctl_poll(ctx);
-  *iters = c.iter;
-  return st;
-}
+  int graphed = -1;  // -1: not captured yet
+  bool fused_dot = false;
+
+  pdeb200_status run(Context* ctx, HierT& H, const GridDev& g, const Coef& cf, const T* b, T* x, int max_iter,
+                     double tol, const pdeb200_options* o, int* iters) {
+    const long long n = g.n;
+    if (!buf.bytes()) buf = Buf(sizeof(T) * n * 3, ctx->stream);
+    T* B = buf.template as<T>();
+    T *r = B, *p = B + n, *q = B + 2 * n;
+    PDEB_CUDA(cudaMemsetAsync(B, 0, sizeof(T) * n * 3, ctx->stream));
+    PDEB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, ctx->stream));
+    PDEB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctl_init(ctx, max_iter, tol, 1e-300);
+    Ctl* C = ctx->d_ctl;
+    const int nb = vec_blocks(n, ctx);
+    k_dot<T, PostBB><<<nb, 256, 0, ctx->stream>>>(n, b, b, ctx->slot(), PostBB{C}, C);
+    T* z = H.z();
+    H.vcycle(ctx, r, C);
+    k_dot<T, PostRZ><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostRZ{C}, C);
+    k_cg_p<T><<<nb, 256, 0, ctx->stream>>>(n, p, z, C, 1);
+    ctx->count(3);
+    const dim3 grid = stencil_grid_auto(g), block = stencil_block();
+    auto iterate = [&](int) {
+      k_apply_folded<Coef, T, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(), PostAlpha{C}, C);
+      k_cg_xr<T, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, x, r, p, q, ctx->slot(), PostRRRel{C}, C);
+      // beta from r.z summed by the preconditioner's last colour passes when it can
+      if (!H.vcycle_dot(ctx, r, C, ctx->slot())) {
+        k_dot<T, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{C}, C);
+        ctx->count();
+      }
+      k_cg_p<T><<<nb, 256, 0, ctx->stream>>>(n, p, z, C, 0);
+      ctx->count(3);
+    };
+    if (graphed < 0) graphed = graph.capture(ctx, iterate) ? 1 : 0;
+    auto step = [&](int it) {
+      if (graphed)
+        graph.launch(ctx);
+      else
+        iterate(it);
+    };
+    pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
+    const Ctl c = ctl_poll(ctx);
+    *iters = c.iter;
+    return st;
+  }
+};
 
 // FP64 iterative refinement around an FP32 MG-preconditioned Krylov solve:
 // r = b - A x in FP64; e = solve(A e = r/|r|) in FP32 to inner_tol; x += |r| e.
@@ -754,6 +766,7 @@ pdeb200_status mixed_refinement(Context* ctx, DevProblem& P, const Coef& cf, con
     double rel = 1.0;
     auto run = [&](auto& H) {
       using HT = std::decay_t<decltype(H)>;
+      MgPcgCore<typename L::F32, HT, float> pcg;
       for (outer = 0; outer < max_outer; ++outer) {
         k_residual_folded<Coef, double, double, 1, PostRRtoAux><<<grid, block, 0, ctx->stream>>>(
             g, cf, d_x, bf, r, ctx->slot(), PostRRtoAux{C}, nullptr);
@@ -777,7 +790,7 @@ pdeb200_status mixed_refinement(Context* ctx, DevProblem& P, const Coef& cf, con
         if (nonsym)
           is = mg_bicgstab_core<typename L::F32, HT, float>(ctx, H, g, cf32, r32, e32, io.max_iter, io.tol, &io, &it);
         else
-          is = mg_pcg_core<typename L::F32, HT, float>(ctx, H, g, cf32, r32, e32, io.max_iter, io.tol, &io, &it);
+          is = pcg.run(ctx, H, g, cf32, r32, e32, io.max_iter, io.tol, &io, &it);
         total_inner += it;
         if (is == PDEB200_ERR_BREAKDOWN && it == 0) {
           st = PDEB200_ERR_BREAKDOWN;
