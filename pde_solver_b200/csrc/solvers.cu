@@ -174,7 +174,8 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
     else
       iterate(it);
   };
-  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false);
+  // |r|^2 <= tol2 on the device (PostRRRel): batches sized by the observed reduction rate
+  pdeb200_status st = drive(ctx, o, max_iter + 1, step, false, true);
   const Ctl c = ctl_poll(ctx);
   if (rep) {
     rep->iterations = c.iter;

@@ -3,6 +3,7 @@
 // its V-cycle, right-hand-side builders and residual reports.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -177,11 +178,18 @@ inline void ctl_set_done(Context* ctx, int status) {
 
 // Enqueue iterations in growing batches and poll; `iterate()` enqueues one
 // iteration. Returns when the device reports done/stop or the cancel flag is set.
+// predict: the iterations monitor |r|^2 against tol2 (relative rule); after two
+// polls the next batch is the number of iterations the observed reduction
+// rate still needs, so few iterations are enqueued past convergence (they
+// would return at once, but each still costs its launches).
 template <class It>
-pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& iterate, bool use_stop) {
+pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& iterate, bool use_stop,
+                     bool predict = false) {
   int enq = 0;
   int batch = 1;
   const int cap = o->check_interval > 0 ? o->check_interval : 16;
+  double rr_prev = -1.0;
+  int it_prev = 0;
   while (true) {
     for (int b = 0; b < batch && enq < max_iter; ++b, ++enq) iterate(enq);
     const Ctl& c = ctl_poll(ctx);
@@ -191,7 +199,17 @@ pdeb200_status drive(Context* ctx, const pdeb200_options* o, int max_iter, It&& 
       ctl_set_done(ctx, PDEB200_ERR_CANCELLED);
       return PDEB200_ERR_CANCELLED;
     }
-    batch = batch * 2 < cap ? batch * 2 : cap;
+    int next = batch * 2 < cap ? batch * 2 : cap;
+    if (predict && c.rr > 0.0 && c.tol2 > 0.0) {
+      if (rr_prev > 0.0 && c.iter > it_prev && c.rr < rr_prev) {
+        const double rate = std::log(c.rr / rr_prev) / double(c.iter - it_prev);  // < 0
+        const double need = std::log(c.tol2 / c.rr) / rate;
+        if (need > 0.0 && need < double(cap)) next = std::max(1, (int)std::ceil(need));
+      }
+      rr_prev = c.rr;
+      it_prev = c.iter;
+    }
+    batch = next;
   }
 }
 
