@@ -4,7 +4,7 @@
 Tolerances: the reference methods run the reference's algorithm, so fields
 agree to rounding (rel L2 <= 1e-10; FMA contraction on the GPU is the only
 difference). The MG-PCG form solves the folded system to 1e-12 relative
-residual on both sides and must agree to <= 1e-9 rel L2 (north_star bar)."""
+residual on both sides and must agree to <= 1e-9 rel L2 (the plain FP64 path's parity bar)."""
 import numpy as np
 import pytest
 
