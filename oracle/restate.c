@@ -1,7 +1,7 @@
 /* Test infrastructure only (the oracle): plain-C restatement of the
- * reference's structured-grid solve path. It is the checker of libpdeb200.so
- * in tests/, smoke() and the CPU baseline of bench.py; nothing in the product
- * links or calls it.
+ * reference's structured-grid solve path. tests/, smoke() and the CPU
+ * baseline of bench.py compare libpdeb200.so against it; nothing in the
+ * product links or calls it.
  *
  * Expression order follows the reference line by line where the reference
  * has the computation, so that the restatement reproduces oracle/_ref
