@@ -849,6 +849,75 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict_fold(GridDev gc, TC* __re
   }
 }
 
+// The fold of k_restrict_fold on the face-adjacent interior nodes only, one
+// thread per node: the nodes are enumerated layer by layer (i = 1, i = nx-2,
+// j = 1, j = ny-2, k = 1, k = nz-2), each layer without the nodes of the
+// layers before it, so every node is visited once. Same arithmetic per node.
+struct FoldLayers {
+  long long start[7];  // prefix counts of the six layers
+};
+
+inline FoldLayers fold_layers(const GridDev& g) {
+  FoldLayers L{};
+  const long long ni = g.nx - 2, nj = g.ny - 2, nk = g.dim == 3 ? g.nz - 2 : 1;
+  const long long mi = ni > 2 ? ni - 2 : 0, mj = nj > 2 ? nj - 2 : 0;  // i (j) not on an x (y) layer
+  long long c[6];
+  c[0] = nj * nk;                               // i = 1
+  c[1] = ni > 1 ? nj * nk : 0;                  // i = nx-2
+  c[2] = mi * nk;                               // j = 1
+  c[3] = nj > 1 ? mi * nk : 0;                  // j = ny-2
+  c[4] = g.dim == 3 ? mi * mj : 0;              // k = 1
+  c[5] = g.dim == 3 && nk > 1 ? mi * mj : 0;    // k = nz-2
+  L.start[0] = 0;
+  for (int q = 0; q < 6; ++q) L.start[q + 1] = L.start[q] + c[q];
+  return L;
+}
+
+template <typename TC>
+__global__ void __launch_bounds__(256) k_restrict_fold_faces(GridDev gc, FoldLayers lay, TC* __restrict__ bc,
+                                                             const Ctl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const long long ni = gc.nx - 2, nj = gc.ny - 2;
+  const long long mi = ni > 2 ? ni - 2 : 0;
+  const int kb = gc.dim == 3 ? 1 : 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < lay.start[6];
+       t += (long long)gridDim.x * blockDim.x) {
+    int q = 0;
+    while (t >= lay.start[q + 1]) ++q;
+    const long long u = t - lay.start[q];
+    int I, J, K;
+    if (q <= 1) {  // x layers: all interior (j, k)
+      I = q == 0 ? 1 : gc.nx - 2;
+      J = 1 + int(u % nj);
+      K = kb + int(u / nj);
+    } else if (q <= 3) {  // y layers: i off the x layers, all interior k
+      J = q == 2 ? 1 : gc.ny - 2;
+      I = 2 + int(u % mi);
+      K = kb + int(u / mi);
+    } else {  // z layers: i and j off the x and y layers
+      K = q == 4 ? 1 : gc.nz - 2;
+      I = 2 + int(u % mi);
+      J = 2 + int(u / mi);
+    }
+    const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
+    const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
+    const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
+    double acc = 0.0;
+    for (int dk = dzl; dk <= dzh; ++dk)
+      for (int dj = dyl; dj <= dyh; ++dj)
+        for (int di = dxl; di <= dxh; ++di) {
+          if (di == 0 && dj == 0 && dk == 0) continue;
+          int ci = I + di, cj = J + dj, ck = K + dk;
+          const double coef = ext_chain(gc, ci, cj, ck);
+          if (coef != 0.0 && ci == I && cj == J && ck == K) acc += coef * double(bc[cidx(gc, I + di, J + dj, K + dk)]);
+        }
+    if (acc != 0.0) {
+      const long long id = cidx(gc, I, J, K);
+      bc[id] = TC(double(bc[id]) + acc);
+    }
+  }
+}
+
 // coarse correction value at any coarse node, boundary nodes by the
 // homogeneous closure chain
 template <typename TC>

@@ -708,7 +708,9 @@ struct Hierarchy {
     }
     if (needs_fold) {
       ProfScope ps(ctx, "restrict_fold", l, 0.0);
-      k_restrict_fold<T><<<stencil_grid_auto(C.g), stencil_block(), 0, ctx->stream>>>(C.g, C.b, ctl);
+      const FoldLayers lay = fold_layers(C.g);
+      const int blocks = (int)std::max<long long>(1, std::min<long long>((lay.start[6] + 255) / 256, 148LL * 16));
+      k_restrict_fold_faces<T><<<blocks, 256, 0, ctx->stream>>>(C.g, lay, C.b, ctl);
       ctx->count();
     }
     ctx->count(2);
