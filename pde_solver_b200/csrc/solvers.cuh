@@ -701,8 +701,10 @@ struct Hierarchy {
     {
       ProfScope ps(ctx, "restrict", l, dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
       if (z_nested(L.g, C.g))
-        k_restrict_march<T, T><<<stencil_grid_full(C.g, 8), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b,
-                                                                                                  ctl);
+        // 8 coarse planes per thread share plane sums on large levels; small
+        // levels take one plane per thread (latency rather than bytes)
+        k_restrict_march<T, T><<<stencil_grid_full(C.g, C.g.n > (1LL << 20) ? 8 : 1), stencil_block(), 0,
+                                 ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
       else
         k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
     }
