@@ -11,8 +11,6 @@
 // converged iteration.
 #pragma once
 
-#include <cooperative_groups.h>
-
 #include "device.cuh"
 
 namespace pdeb {
@@ -1266,19 +1264,6 @@ struct TailLevel {
 constexpr int kTailThreads = 512;
 constexpr int kTailMaxLevels = 8;
 
-// The tail runs as one block, or as one thread-block cluster (grid = one
-// cluster): work is spread over every thread of the launch and the phases are
-// separated by the cluster barrier, which orders the global-memory writes of
-// one phase before the reads of the next for all blocks of the cluster.
-__device__ __forceinline__ int tail_tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
-__device__ __forceinline__ int tail_nthreads() { return gridDim.x * blockDim.x; }
-__device__ __forceinline__ void tail_sync() {
-  if (gridDim.x > 1)
-    cooperative_groups::this_cluster().sync();
-  else
-    __syncthreads();
-}
-
 template <class Coef, typename T>
 __device__ __forceinline__ void tail_decode(const GridDev& g, int t, int& i, int& j, int& k) {
   const int ni = g.nx - 2, nj = g.ny - 2;
@@ -1295,7 +1280,7 @@ __device__ void tail_sweeps(const TailLevel<Coef, T>& L, const T* b, int sweeps,
   for (int s = 0; s < sweeps; ++s)
     for (int half = 0; half < 2; ++half) {
       const int color = first ^ half;
-      for (int t = tail_tid(); t < total; t += tail_nthreads()) {
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
         int i, j, k;
         tail_decode<Coef, T>(g, t, i, j, k);
         if (((i + j + k) & 1) != color) continue;
@@ -1306,14 +1291,14 @@ __device__ void tail_sweeps(const TailLevel<Coef, T>& L, const T* b, int sweeps,
         const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
         x[id] = (T(b[id]) - nb_sum<T>(st, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / st.c;
       }
-      tail_sync();
+      __syncthreads();
     }
 }
 
 template <class Coef, typename T>
 __device__ void tail_zero(const TailLevel<Coef, T>& L) {
-  for (long long t = tail_tid(); t < L.g.n; t += tail_nthreads()) L.x[t] = T(0);
-  tail_sync();
+  for (long long t = threadIdx.x; t < L.g.n; t += blockDim.x) L.x[t] = T(0);
+  __syncthreads();
 }
 
 template <class Coef, typename T>
@@ -1329,7 +1314,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
     tail_zero(L);
     tail_sweeps(L, b, pre, 0);
     const int total = (g.nx - 2) * (g.ny - 2) * (g.dim == 3 ? g.nz - 2 : 1);
-    for (int t = tail_tid(); t < total; t += tail_nthreads()) {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
       int i, j, k;
       tail_decode<Coef, T>(g, t, i, j, k);
       const long long id = ((long long)k * g.ny + j) * g.nx + i;
@@ -1341,20 +1326,20 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
       L.r[id] = T(b[id]) - (s.c * x[id] + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm,
                                                     g.dim));
     }
-    tail_sync();
+    __syncthreads();
     const TailLevel<Coef, T>& C = lv[l + 1];
     const GridDev& gc = C.g;
-    for (long long t = tail_tid(); t < gc.n; t += tail_nthreads()) {
+    for (long long t = threadIdx.x; t < gc.n; t += blockDim.x) {
       const int I = int(t % gc.nx), J = int((t / gc.nx) % gc.ny), K = int(t / gc.sxy);
       C.b[t] = T(full_weight<T>(g, gc, L.r, I, J, K));
     }
-    tail_sync();
+    __syncthreads();
     if (fold) {
       const int ctotal = (gc.nx - 2) * (gc.ny - 2) * (gc.dim == 3 ? gc.nz - 2 : 1);
       // each interior coarse node next to a face gathers the boundary values
       // whose closure chain ends at it; writes go to interior nodes only and
       // reads to boundary nodes only, so one pass is race free
-      for (int t = tail_tid(); t < ctotal; t += tail_nthreads()) {
+      for (int t = threadIdx.x; t < ctotal; t += blockDim.x) {
         int I, J, K;
         tail_decode<Coef, T>(gc, t, I, J, K);
         const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
@@ -1376,7 +1361,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
           C.b[id] = T(double(C.b[id]) + acc);
         }
       }
-      tail_sync();
+      __syncthreads();
     }
   }
   // coarsest level: sweeps from zero. With a single interior node (3 nodes a
@@ -1399,7 +1384,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
     const int xmode = map_mode(gf.nx, gc.nx), ymode = map_mode(gf.ny, gc.ny);
     const int zmode = gf.dim == 3 ? map_mode(gf.nz, gc.nz) : 0;
     const int total = (gf.nx - 2) * (gf.ny - 2) * (gf.dim == 3 ? gf.nz - 2 : 1);
-    for (int t = tail_tid(); t < total; t += tail_nthreads()) {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
       int i, j, k;
       tail_decode<Coef, T>(gf, t, i, j, k);
       int I0, J0, K0 = 0;
@@ -1420,7 +1405,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel
       const long long id = ((long long)k * gf.ny + j) * gf.nx + i;
       F.x[id] = T(double(F.x[id]) + v);
     }
-    tail_sync();
+    __syncthreads();
     tail_sweeps(F, l == 0 ? rhs0 : F.b, post, 1);
   }
 }

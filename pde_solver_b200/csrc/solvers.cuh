@@ -496,49 +496,10 @@ struct Hierarchy {
     return p;
   }
 
-  // Levels from tail_l0 down run as one launch (k_tail_vcycle): one block for
-  // levels of at most kTailMaxNodes nodes, or one cluster of tail_cluster
-  // blocks for levels of at most kTailClusterNodes nodes.
+  // Levels from tail_l0 down run as one single-block launch (k_tail_vcycle).
   static constexpr long long kTailMaxNodes = 1100;
-  static constexpr long long kTailClusterNodes = 5000;  // 17^3; 33^3 measured no faster, 65^3 slower
   int tail_l0 = -1;
-  int tail_cluster = 1;
   TailLevel<Coef, T>* d_tail = nullptr;
-
-  // Blocks of the tail's cluster on this device: 16 where the device runs a
-  // cluster of 16 tail blocks, else 8, else 1 (one block). Asked once per
-  // instantiation and device.
-  static int tail_cluster_size(Context* ctx) {
-    static int cached[64] = {0};
-    const int dv = ctx->dev >= 0 && ctx->dev < 64 ? ctx->dev : 0;
-    if (cached[dv]) return cached[dv];
-    int best = 1;
-    for (int cl : {16, 8}) {
-      if (cl > 8 && cudaFuncSetAttribute(k_tail_vcycle<Coef, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                        cudaSuccess) {
-        cudaGetLastError();
-        continue;
-      }
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(cl, 1, 1);
-      cfg.blockDim = dim3(kTailThreads, 1, 1);
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = cl;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, k_tail_vcycle<Coef, T>, &cfg) == cudaSuccess && clusters >= 1) {
-        best = cl;
-        break;
-      }
-      cudaGetLastError();
-    }
-    cached[dv] = best;
-    return best;
-  }
 
   bool coarse_in_smem(const Level& L) const {
     const long long interior = (long long)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.dim == 3 ? L.g.nz - 2 : 1);
@@ -588,15 +549,10 @@ struct Hierarchy {
     // single-block tail: the first level small enough, with at most
     // kTailMaxLevels levels below it (colour-pass form only)
     tail_l0 = -1;
-    tail_cluster = 1;
     if (!fused && std::getenv("PDEB200_NO_TAIL") == nullptr) {
-      const int cl = std::getenv("PDEB200_TAIL_SINGLE") ? 1 : tail_cluster_size(ctx);
-      const long long lim = cl > 1 ? kTailClusterNodes : kTailMaxNodes;
       for (size_t l = 0; l < levels.size(); ++l)
-        if (levels[l].g.n <= lim && (int)(levels.size() - l) <= kTailMaxLevels) {
+        if (levels[l].g.n <= kTailMaxNodes && (int)(levels.size() - l) <= kTailMaxLevels) {
           tail_l0 = (int)l;
-          // a cluster only where the first tail level is larger than one block's share
-          tail_cluster = levels[l].g.n > kTailMaxNodes ? cl : 1;
           break;
         }
     }
@@ -714,25 +670,8 @@ struct Hierarchy {
     const double dofs = interior_dofs(L.g);
     if (l == tail_l0) {
       ProfScope ps(ctx, "tail_vcycle", l, 0.0);
-      if (tail_cluster > 1) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(tail_cluster, 1, 1);
-        cfg.blockDim = dim3(kTailThreads, 1, 1);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = ctx->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = tail_cluster;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        PDEB_CUDA(cudaLaunchKernelEx(&cfg, k_tail_vcycle<Coef, T>, (const TailLevel<Coef, T>*)d_tail,
-                                     (int)levels.size() - l, b, pre, post, coarse_iters, needs_fold ? 1 : 0, ctl));
-      } else {
-        k_tail_vcycle<Coef, T><<<1, kTailThreads, 0, ctx->stream>>>(d_tail, (int)levels.size() - l, b, pre, post,
-                                                                      coarse_iters, needs_fold ? 1 : 0, ctl);
-      }
+      k_tail_vcycle<Coef, T><<<1, kTailThreads, 0, ctx->stream>>>(d_tail, (int)levels.size() - l, b, pre, post,
+                                                                    coarse_iters, needs_fold ? 1 : 0, ctl);
       ctx->count();
       return;
     }
