@@ -803,9 +803,10 @@ __device__ __forceinline__ double full_weight(const GridDev& gf, const GridDev& 
 // Restriction R = Ext^T P^T / 2^dim, in two race-free launches:
 //  k_restrict_fw   full weighting of the fine residual at every coarse node,
 //                  boundary nodes included (one thread per coarse node);
-//  k_restrict_fold interior coarse nodes next to a Neumann/Robin face add
-//                  coef * value of each boundary node whose closure chain ends
-//                  at them (the transpose of the extended prolongation below).
+//  k_restrict_fold_faces  interior coarse nodes next to a Neumann/Robin face
+//                  add coef * value of each boundary node whose closure chain
+//                  ends at them (the transpose of the extended prolongation
+//                  below).
 // Boundary entries of the coarse right-hand side are left holding their full
 // weights; no coarse kernel reads them.
 template <typename T, typename TC>
@@ -820,39 +821,11 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict_fw(GridDev gf, GridDev gc
   for (int K = K0; K < K1; ++K) bc[cidx(gc, I, J, K)] = TC(full_weight<T>(gf, gc, rf, I, J, K));
 }
 
-template <typename TC>
-__global__ void __launch_bounds__(kBx* kBy) k_restrict_fold(GridDev gc, TC* __restrict__ bc, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
-  const int I = blockIdx.x * kBx + threadIdx.x;
-  const int J = blockIdx.y * kBy + threadIdx.y;
-  int K0, K1;
-  column_range(gc, K0, K1);
-  if (!(I >= 1 && I <= gc.nx - 2 && J >= 1 && J <= gc.ny - 2)) return;
-  const int dxl = I == 1 ? -1 : 0, dxh = I == gc.nx - 2 ? 1 : 0;
-  const int dyl = J == 1 ? -1 : 0, dyh = J == gc.ny - 2 ? 1 : 0;
-  for (int K = K0; K < K1; ++K) {
-    const int dzl = gc.dim == 3 && K == 1 ? -1 : 0, dzh = gc.dim == 3 && K == gc.nz - 2 ? 1 : 0;
-    if (dxl == 0 && dxh == 0 && dyl == 0 && dyh == 0 && dzl == 0 && dzh == 0) continue;
-    double acc = 0.0;
-    for (int dk = dzl; dk <= dzh; ++dk)
-      for (int dj = dyl; dj <= dyh; ++dj)
-        for (int di = dxl; di <= dxh; ++di) {
-          if (di == 0 && dj == 0 && dk == 0) continue;
-          int ci = I + di, cj = J + dj, ck = K + dk;
-          const double coef = ext_chain(gc, ci, cj, ck);
-          if (coef != 0.0 && ci == I && cj == J && ck == K) acc += coef * double(bc[cidx(gc, I + di, J + dj, K + dk)]);
-        }
-    if (acc != 0.0) {
-      const long long id = cidx(gc, I, J, K);
-      bc[id] = TC(double(bc[id]) + acc);
-    }
-  }
-}
-
-// The fold of k_restrict_fold on the face-adjacent interior nodes only, one
-// thread per node: the nodes are enumerated layer by layer (i = 1, i = nx-2,
-// j = 1, j = ny-2, k = 1, k = nz-2), each layer without the nodes of the
-// layers before it, so every node is visited once. Same arithmetic per node.
+// The fold on the face-adjacent interior coarse nodes, one thread per node:
+// the nodes are enumerated layer by layer (i = 1, i = nx-2, j = 1, j = ny-2,
+// k = 1, k = nz-2), each layer without the nodes of the layers before it, so
+// every node is visited once; reads go to boundary nodes only and writes to
+// interior nodes only, so one launch is race free.
 struct FoldLayers {
   long long start[7];  // prefix counts of the six layers
 };
@@ -1250,7 +1223,7 @@ __global__ void k_coarse_solve_smem(GridDev g, Coef cf, const TB* __restrict__ b
 // prolongation-add of the extended correction and `post` sweeps (colour order
 // reversed), and `coarse_iters` sweeps from zero on the coarsest level. The
 // arithmetic of every node update is that of k_rbgs / k_residual_folded /
-// full_weight / k_restrict_fold / k_prolong_add. rhs0 is the right-hand side of
+// full_weight / k_restrict_fold_faces / k_prolong_add. rhs0 is the right-hand side of
 // level 0 of the tail; the result is left in lv[0].x.
 template <class Coef, typename T>
 struct TailLevel {
