@@ -109,9 +109,11 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, c
   if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
 }
 
-// r = b - A_fold x on interior nodes, optional fused |r|^2.
+// r = b - A_fold x on interior nodes, optional fused |r|^2. Capped at 64
+// registers (4 blocks/SM; 16 bytes spill): 138 -> 133 us at 257^3. The same cap
+// on k_apply_folded spills 88 bytes and is slower.
 template <class Coef, typename T, typename TB, int NV, class Post>
-__global__ void __launch_bounds__(kBx* kBy) k_residual_folded(GridDev g, Coef cf, const T* __restrict__ x,
+__global__ void __launch_bounds__(kBx* kBy, 4) k_residual_folded(GridDev g, Coef cf, const T* __restrict__ x,
                                                               const TB* __restrict__ b, T* __restrict__ r,
                                                               RedSlot slot, Post post, const Ctl* ctl) {
   if (ctl_skip(ctl)) return;
