@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -328,10 +329,12 @@ def bench_serving(abi, count=256, seed=7):
     for mode, plist in (("device_resident", dprobs), ("host_inputs", probs)):
         res_mode = {}
         # each precision at its best lane setting on this box: mixed groups of
-        # at most 64 requests on 4 lanes, plain FP64 one request per lane on 8
-        for name, prec, lanes in (("mixed", abi.MIXED, 4), ("fp64", abi.FP64, 8)):
-            with Server(lanes=lanes, max_batch=64, precision=prec, tile_x=64, tile_y=64, tile_z=32, pre_smooth=1,
-                        post_smooth=2, inner_tol=1e-5) as s:
+        # at most 64 requests on 4 lanes, plain FP64 one request per lane on 8;
+        # mixed_adaptive solves a request single-grid while fewer than 8 wait
+        for name, prec, lanes, single in (("mixed", abi.MIXED, 4, 0), ("mixed_adaptive", abi.MIXED, 4, 8),
+                                          ("fp64", abi.FP64, 8, 0)):
+            with Server(lanes=lanes, max_batch=64, precision=prec, single_below=single, tile_x=64, tile_y=64,
+                        tile_z=32, pre_smooth=1, post_smooth=2, inner_tol=1e-5) as s:
                 dv = mode == "device_resident"
                 s.wait(s.submit_poisson(plist[0], out=outs[0].data_ptr() if dv else None))
                 s.stats(reset=True)
@@ -343,11 +346,92 @@ def bench_serving(abi, count=256, seed=7):
             res_mode[name] = {"solves_per_s": len(plist) / wall, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
                               "lanes": lanes,
                               "failed": int(sum(r.status != abi.OK for r in res)),
-                              "max_group": int(max(r.group_size for r in res))}
+                              "max_group": int(max(r.group_size for r in res)),
+                              "single_grid": int(sum(r.group_size == 1 for r in res))}
         res_mode["speedup_mixed_vs_fp64"] = res_mode["mixed"]["solves_per_s"] / res_mode["fp64"]["solves_per_s"]
+        res_mode["speedup_mixed_adaptive_vs_fp64"] = (res_mode["mixed_adaptive"]["solves_per_s"] /
+                                                      res_mode["fp64"]["solves_per_s"])
         out[mode] = res_mode
     out["workload"] = f"{count} Poisson requests at saturation (2D 65..513, 3D 65..129), tol 1e-10"
     return out
+
+
+def _pct(xs, q):
+    """Nearest-rank percentile."""
+    xs = sorted(xs)
+    if not xs:
+        return None
+    return xs[min(len(xs) - 1, max(0, math.ceil(q / 100.0 * len(xs)) - 1))]
+
+
+def bench_serving_stream(abi, rates=(50.0, 100.0, 200.0), count=64, seed=11):
+    """Serving stream with a seeded rate sweep: at each rate, `count` requests
+    with Poisson-process arrivals, each submitted at its arrival time, mixing
+    Poisson solves (60 %: 2D sides 65..513, 3D sides 65..129, tol 1e-10),
+    200-step explicit heat runs (25 %: 2D sides 65..257, dt 0.9x the
+    forward-Euler limit) and 2D pressure projections (15 %: 256^2..1024^2,
+    CG to 1e-10); host inputs and outputs. Per rate and precision: completed
+    requests/s over the run, p50/p99 latency (arrival -> result in host
+    memory) over all requests and over the Poisson requests alone, and the
+    peak HBM the server held."""
+    from pde_solver_b200 import synthetic
+    from pde_solver_b200.server import Server
+
+    points = []
+    for rate in rates:
+        items = []
+        for t, kind, sp in synthetic.serving_requests(count, seed=seed, rate_hz=rate):
+            if kind == "poisson":
+                items.append((t, kind, synthetic.poisson_request_problem(sp["n"], sp["dim"], sp["seed"])))
+            elif kind == "heat":
+                items.append((t, kind, synthetic.heat_problem(sp["n"])))
+            else:
+                u, v, p0 = synthetic.projection_fields(sp["n"], sp["seed"])
+                items.append((t, kind, (u, v, p0, sp["n"])))
+        kinds = {k: sum(1 for _, kk, _ in items if kk == k) for k in ("poisson", "heat", "projection")}
+        point = {"rate_hz": rate, "requests": count, "kinds": kinds, "span_s": items[-1][0]}
+        # mixed: every Poisson request batched; mixed_adaptive: while fewer than
+        # 8 Poisson requests wait, each runs single-grid mixed on a free lane
+        for name, prec, lanes, single in (("mixed", abi.MIXED, 4, 0), ("mixed_adaptive", abi.MIXED, 4, 8),
+                                          ("fp64", abi.FP64, 8, 0)):
+            with Server(lanes=lanes, max_batch=64, precision=prec, single_below=single, tile_x=64, tile_y=64,
+                        tile_z=32, pre_smooth=1, post_smooth=2, inner_tol=1e-5) as s:
+
+                def submit(kind, x):
+                    if kind == "poisson":
+                        return s.submit_poisson(x)
+                    if kind == "heat":
+                        return s.submit_heat(x[0], x[1], 200)
+                    u, v, p0, n = x
+                    h = 1.0 / (n - 1)
+                    return s.submit_projection(u, v, None, p0, n, n, 1, h, h, 1.0, 0.01)
+
+                # one request of each kind before the clock starts
+                for kind in ("poisson", "heat", "projection"):
+                    first = next((x for _, kk, x in items if kk == kind), None)
+                    if first is not None:
+                        s.wait(submit(kind, first))
+                s.stats(reset=True)
+                ids = []
+                t0 = time.perf_counter()
+                for t, kind, x in items:
+                    delay = t0 + t - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    ids.append((kind, submit(kind, x)))
+                res = [(kind, s.wait(i)[1]) for kind, i in ids]
+                wall = time.perf_counter() - t0
+                st = s.stats()
+            pl = [r.latency_ms for kind, r in res if kind == "poisson"]
+            point[name] = {"requests_per_s": count / wall, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                           "poisson_p50_ms": _pct(pl, 50), "poisson_p99_ms": _pct(pl, 99),
+                           "failed": int(sum(r.status != abi.OK for _, r in res)),
+                           "max_group": int(max(r.group_size for _, r in res)),
+                           "hbm_peak_gb": st.bytes_peak / 1e9, "lanes": lanes, "single_below": single}
+        points.append(point)
+    return {"workload": f"seeded Poisson-process arrivals at {', '.join(f'{r:g}' for r in rates)} requests/s, "
+                        f"{count} requests each: Poisson 60 % / heat 25 % / projection 15 %, host inputs",
+            "points": points}
 
 
 def run_reference(args):
@@ -548,7 +632,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_forms:
         try:
             line["forms"] = {"batched": bench_batched(lib, abi), "serving": bench_serving(abi),
-                             "output": bench_output(out_dev, n)}
+                             "serving_stream": bench_serving_stream(abi), "output": bench_output(out_dev, n)}
         except Exception as exc:  # the forms never block the headline line
             line["forms"] = {"error": str(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -15,8 +15,8 @@
  * request runs the plain FP64 MG-PCG path (pdeb200_solve). Heat runs use the
  * forward-Euler series of pdeb200_time_series; projections use
  * pdeb200_project_velocity's algorithm. A request's result does not depend on
- * what else is in flight: with fixed batch options the same request gives the
- * same bits alone and in any mix. */
+ * what else is in flight: with fixed batch options (and single_below off) the
+ * same request gives the same bits alone and in any mix. */
 #ifndef PDEB200_SERVER_H
 #define PDEB200_SERVER_H
 
@@ -43,7 +43,12 @@ typedef struct {
   int32_t precision;         /* PDEB200_MIXED (batched groups) or PDEB200_FP64 (plain MG-PCG path) */
   int64_t hbm_budget_bytes;  /* admission budget; 0 = 80% of the device's free memory at create */
   int32_t queue_capacity;    /* queued (not yet admitted) requests; 0 = 65536 */
-  int32_t reserved0;
+  int32_t single_below;      /* MIXED: while fewer than this many Poisson requests wait, a free lane
+                                takes one and solves it on its own grid (FP32 MG-PCG inside FP64
+                                refinement, pdeb200_solve with precision MIXED) instead of as a
+                                batched group, so light load pays no batching latency; results then
+                                agree with a batched solve to the tolerance, not bitwise.
+                                0 or 1 = always batch */
   pdeb200_batch_options batch; /* options of the batched groups (autotune is ignored) */
   int32_t reserved[8];
 } pdeb200_server_options;

@@ -214,7 +214,7 @@ class ServerOptions(C.Structure):
         ("precision", C.c_int32),
         ("hbm_budget_bytes", C.c_int64),
         ("queue_capacity", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("single_below", C.c_int32),
         ("batch", BatchOptions),
         ("reserved", C.c_int32 * 8),
     ]

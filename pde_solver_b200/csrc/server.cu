@@ -65,6 +65,7 @@ struct Server {
   int max_batch = 64;
   int precision = PDEB200_MIXED;
   int queue_cap = 65536;
+  int single_below = 0;
   int64_t budget = 0;
   pdeb200_batch_options bopt{};
   std::mutex mu;
@@ -81,12 +82,21 @@ struct Server {
   std::vector<std::thread> threads;
   std::vector<std::unique_ptr<Context>> ctxs;
 
-  // Takes the next admissible work from the queue (caller holds mu).
-  std::vector<SReq*> take() {
+  // Takes the next admissible work from the queue (caller holds mu). `single`
+  // says that a mixed Poisson request is to be solved on its own grid: fewer
+  // than single_below of them wait, so each free lane takes one.
+  std::vector<SReq*> take(bool& single) {
     std::vector<SReq*> got;
+    single = false;
+    if (precision == PDEB200_MIXED && single_below > 1) {
+      int waiting = 0;
+      for (SReq* r : pending)
+        if (r->kind == PDEB200_REQ_POISSON && ++waiting >= single_below) break;
+      single = waiting < single_below;
+    }
     for (auto it = pending.begin(); it != pending.end();) {
       SReq* r = *it;
-      const bool batchable = r->kind == PDEB200_REQ_POISSON && precision == PDEB200_MIXED;
+      const bool batchable = r->kind == PDEB200_REQ_POISSON && precision == PDEB200_MIXED && !single;
       if (!got.empty()) {
         // a group holds mixed-precision Poisson requests of one tolerance
         if (!batchable || r->tol != got.front()->tol || (int)got.size() >= max_batch) {
@@ -125,7 +135,7 @@ struct Server {
   }
 
   void run_group(Context* ctx, std::vector<SReq*>& g);
-  void run_one(Context* ctx, SReq* r);
+  void run_one(Context* ctx, SReq* r, bool mixed);
   void lane(int q);
 };
 
@@ -166,13 +176,14 @@ void Server::run_group(Context* ctx, std::vector<SReq*>& g) {
   pdeb200_batch_destroy(b);
 }
 
-void Server::run_one(Context* ctx, SReq* r) {
+void Server::run_one(Context* ctx, SReq* r, bool mixed) {
   r->res.group_size = 1;
   try {
     if (r->kind == PDEB200_REQ_POISSON) {
       pdeb200_options o;
       pdeb200_default_options(&o);
       o.method = PDEB200_MG_PCG;
+      if (mixed) o.precision = PDEB200_MIXED;
       o.tol = r->tol;
       o.tol_mode = PDEB200_TOL_RELATIVE;
       o.max_iter = 500;
@@ -234,11 +245,12 @@ void Server::lane(int q) {
   Context* ctx = ctxs[q].get();
   for (;;) {
     std::vector<SReq*> work;
+    bool single = false;
     {
       std::unique_lock<std::mutex> lk(mu);
       cv.wait(lk, [&] {
         if (stop) return true;
-        work = take();
+        work = take(single);
         return !work.empty();
       });
       if (stop && work.empty()) return;
@@ -250,10 +262,11 @@ void Server::lane(int q) {
       ++busy;
       busy_peak = std::max(busy_peak, busy);
     }
-    if (work.front()->kind == PDEB200_REQ_POISSON && precision == PDEB200_MIXED)
+    const bool mixed_poisson = work.front()->kind == PDEB200_REQ_POISSON && precision == PDEB200_MIXED;
+    if (mixed_poisson && !single)
       run_group(ctx, work);
     else
-      run_one(ctx, work.front());
+      run_one(ctx, work.front(), mixed_poisson);
     {
       std::lock_guard<std::mutex> lk(mu);
       for (auto* r : work) finish(r);
@@ -333,6 +346,7 @@ pdeb200_status pdeb200_server_create(const pdeb200_server_options* opt, pdeb200_
     S.max_batch = opt->max_batch > 0 ? opt->max_batch : 64;
     S.precision = opt->precision == PDEB200_FP64 ? PDEB200_FP64 : PDEB200_MIXED;
     S.queue_cap = opt->queue_capacity > 0 ? opt->queue_capacity : 65536;
+    S.single_below = opt->single_below;
     S.bopt = opt->batch;
     size_t fr = 0, tot = 0;
     PDEB_CUDA(cudaMemGetInfo(&fr, &tot));
@@ -393,7 +407,9 @@ pdeb200_status pdeb200_server_submit(pdeb200_server* h, const pdeb200_request* r
   } else {
     return PDEB200_ERR_INVALID;
   }
-  r->bytes = estimate_bytes(*r, S.precision);
+  // a mixed request that may run on its own grid is admitted at the FP64
+  // path's estimate, which bounds the single-grid mixed working set
+  r->bytes = estimate_bytes(*r, S.precision == PDEB200_MIXED && S.single_below > 1 ? PDEB200_FP64 : S.precision);
   std::lock_guard<std::mutex> lk(S.mu);
   if (r->bytes > S.budget) {
     ++S.rejected;

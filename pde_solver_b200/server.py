@@ -30,11 +30,12 @@ def _dp(a):
 
 class Server:
     def __init__(self, lanes=4, max_batch=64, precision=abi.MIXED, hbm_budget_bytes=0, device=0,
-                 queue_capacity=0, **batch_kw):
+                 queue_capacity=0, single_below=0, **batch_kw):
         self.lib = abi.load()
         o = abi.ServerOptions()
         o.device, o.lanes, o.max_batch, o.precision = device, lanes, max_batch, precision
         o.hbm_budget_bytes, o.queue_capacity = hbm_budget_bytes, queue_capacity
+        o.single_below = single_below
         o.batch = batch_default_options(**batch_kw)
         self._h = C.c_void_p()
         msg = C.create_string_buffer(512)

@@ -88,6 +88,26 @@ def test_each_result_same_alone_and_in_the_mix():
         assert np.array_equal(got[k][0], ref), k
 
 
+def test_light_load_runs_single_grid_mixed(oracle_mod):
+    # with single_below set, a Poisson request that waits alone runs on its own
+    # grid in mixed precision: the bits of pdeb200_solve with precision MIXED,
+    # FP64 residual <= 1e-10 by the oracle's operator, and within 1e-8 of the
+    # batched result of the same request
+    ps = poisson_mix()[:3]
+    with Server(lanes=2, single_below=4) as s:
+        outs = [s.wait(s.submit_poisson(p)) for p in ps]
+    with Server(lanes=1) as s:
+        batched = [s.wait(s.submit_poisson(p))[0] for p in ps]
+    opt = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=500,
+                          precision=abi.MIXED)
+    for p, (out, res), b in zip(ps, outs, batched):
+        assert res.status == abi.OK and res.group_size == 1 and res.rel_residual <= 1e-10
+        assert folded_rel(oracle_mod, p, out) <= 1.01e-10
+        ref, _ = solver.solve(p, opt)
+        assert np.array_equal(out, ref)
+        assert np.linalg.norm(out - b) <= 1e-8 * np.linalg.norm(b)
+
+
 def test_admission_respects_the_hbm_budget():
     ps = [synthetic.poisson_request_problem(129, 2, seed=q) for q in range(8)]
     one = 80 * ps[0].n + (1 << 20)
