@@ -83,7 +83,10 @@ def ncu_traffic(kernel_name):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region,
+    every 200 ms: a query now and then holds the GPU's work up by tens of ms
+    (measured on the 257^3 solve: about one run in four at 100 ms), so the
+    sampling is no denser than the clocks record needs."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -100,7 +103,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -597,9 +600,13 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_dev, step_wall = [], []
     e0.record(stream)
     for _ in range(args.steps):
+        t_step = time.perf_counter()
         rep = solve_dev()
+        step_wall.append((time.perf_counter() - t_step) * 1e3)
+        step_dev.append(rep.device_ms)
         launches += rep.kernel_launches
     e1.record(stream)
     torch.cuda.synchronize()
@@ -678,6 +685,9 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8,
                 "matches_device_result": bool(ok_host)},
         "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
+        # each timed solve: its own device time (events inside the call) and
+        # the host wall time of the call
+        "steps_detail": {"device_ms": [round(v, 3) for v in step_dev], "wall_ms": [round(v, 3) for v in step_wall]},
     }
     if rank == 0 and world == 1 and not args.no_forms:
         forms = {}

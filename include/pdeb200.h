@@ -174,7 +174,8 @@ typedef struct {
   int32_t gs_ordering;       /* pdeb200_ordering for GAUSS_SEIDEL / SOR */
   int32_t device;            /* CUDA device ordinal */
   int32_t check_interval;    /* host convergence poll period (iterations); 0 = auto */
-  double inner_tol;          /* MIXED: relative tolerance of each inner FP32 solve */
+  double inner_tol;          /* MIXED: relative tolerance of each inner FP32 solve (default 1e-5); a
+                                last refinement step asks only the reduction the target needs */
   int32_t bf16_coefficients; /* MIXED: store smoother k in BF16 */
   int32_t max_outer;         /* MIXED: iterative-refinement cap */
   const volatile int32_t* cancel; /* polled between iterations (SolveInput::cancel) */

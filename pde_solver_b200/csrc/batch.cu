@@ -282,6 +282,7 @@ int solve_all(BatchPlan& B, double tol, int max_cycles_cap = 0) {
     M.bb = M.rr0 = M.rr = M.rr_outer = M.rz = M.alpha = M.beta = 0.0;
     M.tol2 = tol * tol;
     M.tol2_inner = B.prm.inner_tol * B.prm.inner_tol;
+    M.tol2_step = M.tol2_inner;
     M.max_inner = B.prm.max_inner;
     M.max_outer = B.prm.max_outer;
   }

@@ -65,6 +65,7 @@ struct BMember {
   double rz, alpha, beta;
   double tol2;        // tol^2 (outer, relative to |b|)
   double tol2_inner;  // inner_tol^2 (relative to rr0)
+  double tol2_step;   // this inner solve's target (relative to rr0): tol2_inner, or looser on a last step
   double* x64;
   double* b64;
   const double* f64;
@@ -261,6 +262,10 @@ struct BPostOuter {
       m->inner = 0;
       m->rr0 = rr;
       m->rr = rr;
+      // the inner solve only has to take |r|^2 from rr to the target: on the
+      // last refinement step that is less than inner_tol (a factor 4 of
+      // margin on |r| for the FP32 operator's rounding)
+      m->tol2_step = fmax(m->tol2_inner, fmin(0.01, 0.0625 * m->tol2 * m->bb / rr));
     }
   }
 };
@@ -288,7 +293,7 @@ struct BPostUpdate {
       return;
     }
     m->e_valid = 1;
-    if (rr <= m->tol2_inner * m->rr0 || m->inner >= m->max_inner) m->state = kBNeedOuter;
+    if (rr <= m->tol2_step * m->rr0 || m->inner >= m->max_inner) m->state = kBNeedOuter;
   }
 };
 

@@ -508,7 +508,7 @@ void pdeb200_default_options(pdeb200_options* o) {
   o->gs_ordering = PDEB200_ORDER_LEXICOGRAPHIC;
   o->device = 0;
   o->check_interval = 0;
-  o->inner_tol = 1e-4;
+  o->inner_tol = 1e-5;
   o->bf16_coefficients = 0;
   o->max_outer = 50;
   o->cancel = nullptr;

@@ -156,7 +156,7 @@ def default_options(lib=None, **kw) -> abi.Options:
     o.gs_ordering = abi.ORDER_LEXICOGRAPHIC
     o.device = 0
     o.check_interval = 0
-    o.inner_tol = 1e-4
+    o.inner_tol = 1e-5
     o.bf16_coefficients = 0
     o.max_outer = 50
     for k, v in kw.items():
