@@ -44,7 +44,8 @@ typedef struct {
   int32_t bf16_coefficients; /* 1: hierarchy k stored as BF16 */
   int32_t no_graph;        /* 1: launch the cycle's kernels directly instead of a graph */
   int32_t autotune;        /* 1: time candidate schedules at create and keep the fastest */
-  double inner_tol;        /* inner relative tolerance; 0 = 1e-4 */
+  double inner_tol;        /* inner relative tolerance; 0 = 1e-4. A member's last refinement step
+                              stops once the reduction left to the target is reached */
   const char* tune_cache;  /* autotuner cache file; NULL = $PDEB200_TUNE_CACHE, else none */
   void* stream;            /* cudaStream_t for all work; NULL = the batch's own stream */
   int32_t no_compact;      /* 1: keep every member's tiles in the launches until the solve ends */
