@@ -303,8 +303,8 @@ def oracle_available():
 def bench_serving(abi, count=256, seed=7):
     """Serving form: a stream of Poisson requests (2D sides 65..513, 3D sides
     65..129, k log-normal sigma=0.5) submitted at once (saturation) to a
-    4-lane server, mixed precision (continuous batching) vs the plain FP64
-    path; latency is submit -> result written to host memory."""
+    server, mixed precision (continuous batching, 6 lanes) vs the plain FP64
+    path (16 lanes); latency is submit -> result written to host memory."""
     from pde_solver_b200 import synthetic
     from pde_solver_b200.server import Server
 
@@ -331,11 +331,12 @@ def bench_serving(abi, count=256, seed=7):
     out = {}
     for mode, plist in (("device_resident", dprobs), ("host_inputs", probs)):
         res_mode = {}
-        # each precision at its best lane setting on this box: mixed groups of
-        # at most 64 requests on 4 lanes, plain FP64 one request per lane on 8;
-        # mixed_adaptive solves a request single-grid while fewer than 8 wait
-        for name, prec, lanes, single in (("mixed", abi.MIXED, 4, 0), ("mixed_adaptive", abi.MIXED, 4, 8),
-                                          ("fp64", abi.FP64, 8, 0)):
+        # each precision at its best lane setting on this box (swept): mixed
+        # groups of at most 64 requests on 6 lanes, plain FP64 one request per
+        # lane on 16; mixed_adaptive solves a request single-grid while fewer
+        # than 8 wait
+        for name, prec, lanes, single in (("mixed", abi.MIXED, 6, 0), ("mixed_adaptive", abi.MIXED, 6, 8),
+                                          ("fp64", abi.FP64, 16, 0)):
             with Server(lanes=lanes, max_batch=64, precision=prec, single_below=single, tile_x=64, tile_y=64,
                         tile_z=32, pre_smooth=1, post_smooth=2, inner_tol=1e-5) as s:
                 dv = mode == "device_resident"
@@ -445,8 +446,8 @@ def bench_serving_stream(abi, rates=(50.0, 100.0, 200.0), count=64, seed=11):
         point = {"rate_hz": rate, "requests": count, "kinds": kinds, "span_s": items[-1][0]}
         # mixed: every Poisson request batched; mixed_adaptive: while fewer than
         # 8 Poisson requests wait, each runs single-grid mixed on a free lane
-        for name, prec, lanes, single in (("mixed", abi.MIXED, 4, 0), ("mixed_adaptive", abi.MIXED, 4, 8),
-                                          ("fp64", abi.FP64, 8, 0)):
+        for name, prec, lanes, single in (("mixed", abi.MIXED, 6, 0), ("mixed_adaptive", abi.MIXED, 6, 8),
+                                          ("fp64", abi.FP64, 16, 0)):
             with Server(lanes=lanes, max_batch=64, precision=prec, single_below=single, tile_x=64, tile_y=64,
                         tile_z=32, pre_smooth=1, post_smooth=2, inner_tol=1e-5) as s:
 
