@@ -701,9 +701,12 @@ struct Hierarchy {
     {
       ProfScope ps(ctx, "restrict", l, dofs * sizeof(T) * (1.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
       if (z_nested(L.g, C.g))
-        // 8 coarse planes per thread share plane sums on large levels; small
-        // levels take one plane per thread (latency rather than bytes)
-        k_restrict_march<T, T><<<stencil_grid_full(C.g, C.g.n > (1LL << 20) ? 8 : 1), stencil_block(), 0,
+        // 4 coarse planes per thread share plane sums on large levels (into
+        // 129^3: 58.3 us, against 61.3 with 8 and 76.0 with 16); small levels
+        // take one plane per thread (latency rather than bytes). The result
+        // does not depend on the chunking: a chunk's first plane sum is
+        // recomputed with the same arithmetic as a carried one.
+        k_restrict_march<T, T><<<stencil_grid_full(C.g, C.g.n > (1LL << 20) ? 4 : 1), stencil_block(), 0,
                                  ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
       else
         k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
