@@ -7,6 +7,11 @@ requests that wait together.
         rid = s.submit_poisson(problem)          # returns at once
         u, res = s.wait(rid)                      # solution and timing record
         print(s.stats().p99_ms)
+
+`single_below=n` (MIXED only): while fewer than n Poisson requests wait, a
+free lane solves one on its own grid in mixed precision instead of as a
+batched group (lower latency at light load; results then agree with a
+batched solve to the tolerance rather than bitwise).
 """
 from __future__ import annotations
 
