@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PDEB200_ABI_VERSION 1
+#define PDEB200_ABI_VERSION 2
 
 typedef enum {
   PDEB200_OK = 0,
@@ -100,6 +100,30 @@ typedef enum {
   PDEB200_COEF_NODAL = 2
 } pdeb200_coef_kind;
 
+/* Pointwise nonlinear terms sum(coeff * g(u)) of the discrete equation
+ * (NonlinearTerm / NonlinearKind, include/pde_types.h:88-100), evaluated at
+ * the node's current value the way EvalNonlinear does
+ * (src/backends/cpu/solvers/relaxation.cpp:27-45, src/backends/cpu/solver.cpp:234-256):
+ * g = u^power, sin u, cos u, exp u or |u|. The relaxation methods (Jacobi,
+ * Gauss-Seidel, SOR), the explicit time series and the residual norms take
+ * them; the Krylov and multigrid methods reject them, as the reference does
+ * (src/backends/cpu/solver.cpp:502,550). */
+#define PDEB200_MAX_NONLINEAR 8
+
+typedef enum {
+  PDEB200_NL_POWER = 0,
+  PDEB200_NL_SIN = 1,
+  PDEB200_NL_COS = 2,
+  PDEB200_NL_EXP = 3,
+  PDEB200_NL_ABS = 4
+} pdeb200_nonlinear_kind;
+
+typedef struct {
+  int32_t kind;   /* pdeb200_nonlinear_kind */
+  int32_t power;  /* NL_POWER exponent */
+  double coeff;
+} pdeb200_nonlinear_term;
+
 /* Where the pointers of a problem live. */
 typedef enum {
   PDEB200_MEM_HOST = 0,   /* host pointers; copies are part of the call */
@@ -120,6 +144,9 @@ typedef struct {
   const double* f;               /* per-node f in the reference sign convention, N values */
   const double* u0;              /* initial field (time series) or initial guess, N values */
   pdeb200_face face[6];
+  int32_t n_nonlinear;           /* 0 .. PDEB200_MAX_NONLINEAR */
+  int32_t reserved2;
+  const pdeb200_nonlinear_term* nonlinear;  /* host array of n_nonlinear terms (any mem_space) */
 } pdeb200_problem;
 
 /* Methods: the first seven are SolveMethod (include/pde_types.h:230-238) with the
@@ -310,11 +337,13 @@ pdeb200_status pdeb200_project_velocity(int32_t nx, int32_t ny, int32_t nz,
  * faces take constant values only, and the solver's scratch (second field,
  * reduction partials, control block) is one file-scope device array of about
  * 8.3 MB that every GPU loading the library keeps until the process exits.
- * Grids above 1048576 nodes are rejected (PDEB200_ERR_UNSUPPORTED). All calls
- * share that array: calls that overlap on the GPU race, so callers serialise
- * them. The first call on a device looks up the array's address (set-up) and
- * should come before any stream capture on that device. `stream` may be NULL
- * (the default stream). */
+ * Grids above 1048576 nodes, or with more than 8192 x-y blocks of 32 x 8
+ * columns (ceil(nx/32)*ceil(ny/8) > 8192, e.g. a long, thin 2D grid), are
+ * rejected (PDEB200_ERR_UNSUPPORTED). All calls share that array: calls that
+ * overlap on the GPU race, so callers serialise them. Every call looks up the
+ * array's address (so a device reset between calls is harmless); the first
+ * call on a device also loads the module there and should come before any
+ * stream capture on that device. `stream` may be NULL (the default stream). */
 pdeb200_status pdeb200_jacobi_noalloc(const pdeb200_problem* prob, int32_t max_iter, double tol,
                                       int32_t device, void* stream, double* out_grid,
                                       pdeb200_report* report);

@@ -25,10 +25,28 @@ P = C.POINTER
 DP = P(C.c_double)
 
 
+def _makefile_ref() -> str:
+    """The reference source tree oracle/Makefile compiles by default (its `REF ?=` line)."""
+    with open(os.path.join(HERE, "Makefile")) as fh:
+        for line in fh:
+            if line.startswith("REF ?="):
+                return line.split("=", 1)[1].strip()
+    return ""
+
+
+# Where the reference's sources lie: $PDE_SOLVER_REF, else the Makefile's default.
+REF_SRC = os.environ.get("PDE_SOLVER_REF") or _makefile_ref()
+
+
+def have_reference_sources() -> bool:
+    """True where the reference's CPU solver sources can be compiled (not on a box without them)."""
+    return bool(REF_SRC) and os.path.exists(os.path.join(REF_SRC, "src", "backends", "cpu", "solver.cpp"))
+
+
 def build(ref: bool = True) -> None:
     """make -C oracle (restatement always; the reference when its sources exist)."""
     target = "all" if ref else "restate"
-    subprocess.run(["make", "-s", "-C", HERE, "-j8", target], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", target, f"REF={REF_SRC}"], check=True)
 
 
 _restate = None

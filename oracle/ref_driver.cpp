@@ -110,6 +110,13 @@ bool BuildInput(const pdeb200_problem* p, const char* rhs_latex, const char* con
     const size_t n = static_cast<size_t>(p->nx) * p->ny * (p->nz <= 1 ? 1 : p->nz);
     in->initial_grid.assign(p->u0, p->u0 + n);
   }
+  for (int t = 0; t < p->n_nonlinear; ++t) {
+    NonlinearTerm nt;
+    nt.kind = static_cast<NonlinearKind>(p->nonlinear[t].kind);
+    nt.coeff = p->nonlinear[t].coeff;
+    nt.power = p->nonlinear[t].power;
+    in->nonlinear.push_back(nt);
+  }
   return true;
 }
 

@@ -170,6 +170,30 @@ static inline double f_at(const Grid* g, long id) {
   return g->p->f ? g->p->f[id] : g->p->f_const;
 }
 
+/* EvalNonlinear (relaxation.cpp:27-45, solver.cpp:234-256): sum of
+ * coeff * g(u) in term order, g = u^power, sin, cos, exp, |u|. */
+static double eval_nonlinear(const pdeb200_problem* p, double u) {
+  double value = 0.0;
+  for (int t = 0; t < p->n_nonlinear; ++t) {
+    const pdeb200_nonlinear_term* nt = &p->nonlinear[t];
+    switch (nt->kind) {
+      case PDEB200_NL_POWER: value += nt->coeff * pow(u, (double)nt->power); break;
+      case PDEB200_NL_SIN: value += nt->coeff * sin(u); break;
+      case PDEB200_NL_COS: value += nt->coeff * cos(u); break;
+      case PDEB200_NL_EXP: value += nt->coeff * exp(u); break;
+      default: value += nt->coeff * fabs(u); break;
+    }
+  }
+  return value;
+}
+
+/* (f + integral) + nonlinear, the reference's sum with no integral term
+ * (relaxation.cpp:281, solver.cpp:948, residual.cpp:487). */
+static inline double f_nl(const Grid* g, long id, double u) {
+  const double f = f_at(g, id);
+  return g->p->n_nonlinear ? f + eval_nonlinear(g->p, u) : f;
+}
+
 /* Neighbour sum in the reference's order (solver.cpp:892-898, cpu_utils.cpp:428-433). */
 static inline double nb_sum(const Grid* g, const Stencil* s, const double* u, long id) {
   double v = s->xp * u[id + 1] + s->xm * u[id - 1] + s->yp * u[id + g->nx] + s->ym * u[id - g->nx];
@@ -299,13 +323,13 @@ static int all_dirichlet(const Grid* g) {
 /* ---------------------------------------------------------- relaxation */
 
 /* One interior point update; returns the new value. Reference expression order:
- * rhs = -(f + 0 + 0 + 0) - (lap + 0 + 0 + 0); upd = rhs/center
+ * rhs = -(f + 0 + nonlinear(old) + 0) - (lap + 0 + 0 + 0); upd = rhs/center
  * (relaxation.cpp:534-536, solver.cpp:955-962). */
 static inline double relax_point(const Grid* g, const double* u, int i, int j, int k, long id) {
   Stencil s;
   node_stencil(g, i, j, k, &s);
   const double lap = nb_sum(g, &s, u, id);
-  const double rhs = -(f_at(g, id)) - (lap);
+  const double rhs = -(f_nl(g, id, u[id])) - (lap);
   return rhs / s.c;
 }
 
@@ -1355,6 +1379,14 @@ int rs_solve(const pdeb200_problem* prob, const pdeb200_options* o, double* out,
     return st;
   }
   double omp0 = omp_get_wtime();
+  if (prob->n_nonlinear > 0 && o->method != PDEB200_JACOBI && o->method != PDEB200_GAUSS_SEIDEL &&
+      o->method != PDEB200_SOR) {
+    /* solver.cpp:502,550 */
+    set_msg(rep, o->method >= PDEB200_CG && o->method <= PDEB200_GMRES ? "Krylov solvers require linear PDEs"
+                                                                      : "Multigrid requires linear PDEs");
+    grid_free(&g);
+    return PDEB200_ERR_UNSUPPORTED;
+  }
   switch (o->method) {
     case PDEB200_JACOBI:
     case PDEB200_GAUSS_SEIDEL:
@@ -1506,7 +1538,7 @@ int rs_residual_norms(const pdeb200_problem* prob, const double* grid, double* l
         }
         Stencil s;
         node_stencil(&g, i, j, 0, &s);
-        const double r = s.c * u + nb_sum(&g, &s, grid, id) + (f_at(&g, id));
+        const double r = s.c * u + nb_sum(&g, &s, grid, id) + (f_nl(&g, id, u));
         ACC(r);
       }
   } else {
@@ -1561,7 +1593,8 @@ int rs_time_series(const pdeb200_problem* prob, const pdeb200_time_options* t, d
       for (int j = 1; j < g.ny - 1; ++j)
         for (int i = 1; i < g.nx - 1; ++i) {
           const long id = ID(&g, i, j, k);
-          const double rhs = opv[id] + f_at(&g, id);
+          const double rhs = g.p->n_nonlinear ? opv[id] + f_at(&g, id) + eval_nonlinear(g.p, grid[id])
+                                              : opv[id] + f_at(&g, id);
           double u_t = 0.0;
           if (fabs(ut) >= 1e-12) {
             u_t = -rhs / ut;

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-PDEB200_ABI_VERSION = 1
+PDEB200_ABI_VERSION = 2
 
 # pdeb200_status
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_CUDA, ERR_OOM = 0, 1, 2, 3, 4, 5
@@ -25,6 +25,9 @@ JACOBI, GAUSS_SEIDEL, SOR, CG, BICGSTAB, GMRES, MG_VCYCLE, MG_PCG, MG_BICGSTAB =
 TOL_REFERENCE, TOL_RELATIVE = 0, 1
 FP64, MIXED = 0, 1
 ORDER_LEXICOGRAPHIC, ORDER_REDBLACK = 0, 1
+# pointwise nonlinear term kinds (NonlinearKind order)
+NL_POWER, NL_SIN, NL_COS, NL_EXP, NL_ABS = range(5)
+MAX_NONLINEAR = 8
 
 FACE_NAMES = ("left", "right", "bottom", "top", "front", "back")
 
@@ -41,6 +44,14 @@ class Face(C.Structure):
         ("alpha_arr", C.POINTER(C.c_double)),
         ("beta_arr", C.POINTER(C.c_double)),
         ("gamma_arr", C.POINTER(C.c_double)),
+    ]
+
+
+class NonlinearTerm(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("power", C.c_int32),
+        ("coeff", C.c_double),
     ]
 
 
@@ -72,6 +83,9 @@ class Problem(C.Structure):
         ("f", C.POINTER(C.c_double)),
         ("u0", C.POINTER(C.c_double)),
         ("face", Face * 6),
+        ("n_nonlinear", C.c_int32),
+        ("reserved2", C.c_int32),
+        ("nonlinear", C.POINTER(NonlinearTerm)),
     ]
 
 

@@ -443,6 +443,7 @@ void create_plan(BatchPlan& B, const pdeb200_problem* probs, int count, const pd
     const pdeb200_problem& hp = probs[m];
     if (hp.coef_kind != PDEB200_COEF_CONST && hp.coef_kind != PDEB200_COEF_DIVK)
       throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "batch members take COEF_CONST or COEF_DIVK"};
+    if (hp.n_nonlinear > 0) throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "Multigrid requires linear PDEs"};
     describe_problem(&B.cx, &hp, &B.probs[m]);
     DevProblem& P = B.probs[m];
     B.off[m] = B.nodes;

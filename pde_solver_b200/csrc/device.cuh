@@ -205,6 +205,46 @@ __device__ __forceinline__ void fold_faces(const GridDev& g, int i, int j, int k
   if (bshift) *bshift = sh;
 }
 
+// Pointwise nonlinear terms sum(coeff * g(u)) (NonlinearTerm,
+// include/pde_types.h:88-100), passed to kernels by value. nl_eval follows
+// EvalNonlinear (src/backends/cpu/solvers/relaxation.cpp:27-45,
+// src/backends/cpu/solver.cpp:234-256): terms summed in order, each product
+// and sum rounded once (no contraction). Integer powers 0, 1 and 2 are exact
+// or one rounding (u*u), which is what a correctly rounded pow gives.
+constexpr int kMaxNonlinear = 8;
+struct NonlinDev {
+  int n;
+  int kind[kMaxNonlinear];
+  int power[kMaxNonlinear];
+  double coeff[kMaxNonlinear];
+};
+
+__device__ __forceinline__ double nl_eval(const NonlinDev& nl, double u) {
+  double v = 0.0;
+  for (int t = 0; t < nl.n; ++t) {
+    double gv;
+    switch (nl.kind[t]) {
+      case 0: {
+        const int p = nl.power[t];
+        gv = p == 0 ? 1.0 : p == 1 ? u : p == 2 ? __dmul_rn(u, u) : pow(u, double(p));
+        break;
+      }
+      case 1: gv = sin(u); break;
+      case 2: gv = cos(u); break;
+      case 3: gv = exp(u); break;
+      default: gv = fabs(u); break;
+    }
+    v = __dadd_rn(v, __dmul_rn(nl.coeff[t], gv));
+  }
+  return v;
+}
+
+// f + nonlinear(u) in the reference's order ((f + integral) + nonlinear, the
+// integral term being absent here); plain f without terms.
+__device__ __forceinline__ double f_plus_nl(double fv, const NonlinDev& nl, double u) {
+  return nl.n ? __dadd_rn(fv, nl_eval(nl, u)) : fv;
+}
+
 // Neighbour sum in the reference's left-to-right order
 // (src/backends/cpu/solver.cpp:892-898, cpu_utils.cpp:428-433).
 template <typename T>

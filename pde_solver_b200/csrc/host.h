@@ -196,6 +196,7 @@ struct DevProblem {
   const double* f = nullptr;
   double f_const = 0.0;
   const double* u0 = nullptr;
+  NonlinDev nl{};  // pointwise nonlinear terms (relaxation, time series, 2D residual norms)
   double dx = 0, dy = 0, dz = 0;
   double a = 0, b = 0, az = 0, c = 0, d = 0, dzc = 0, e = 0, ut = 0;
   std::vector<Buf> owned;

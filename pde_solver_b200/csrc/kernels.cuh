@@ -426,11 +426,12 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_full(GridDev g, Coef cf, con
 // ---------------------------------------------------------------- Jacobi
 
 // One Jacobi sweep of the reference (relaxation.cpp:426-546, solver.cpp:808-962):
-// next = (-f - lap)/center on interior nodes, reading the stored face values of
-// `grid`; fused max|du| (the reference's stopping quantity).
+// next = (-(f + nonlinear(u)) - lap)/center on interior nodes, reading the
+// stored face values of `grid`; fused max|du| (the reference's stopping
+// quantity).
 template <class Coef, class Post>
 __global__ void __launch_bounds__(kBx* kBy) k_jacobi(GridDev g, Coef cf, const double* __restrict__ f,
-                                                     double f_const, const double* __restrict__ grid,
+                                                     double f_const, NonlinDev nl, const double* __restrict__ grid,
                                                      double* __restrict__ next, RedSlot slot, Post post,
                                                      const Ctl* ctl, int* degenerate) {
   if (ctl_stopped(ctl)) return;
@@ -450,10 +451,11 @@ __global__ void __launch_bounds__(kBx* kBy) k_jacobi(GridDev g, Coef cf, const d
       const double zp = g.dim == 3 ? grid[id + g.sxy] : 0.0;
       const double zm = g.dim == 3 ? grid[id - g.sxy] : 0.0;
       const double lap = nb_sum<double>(s, grid[id + 1], grid[id - 1], grid[id + g.nx], grid[id - g.nx], zp, zm, g.dim);
-      const double rhs = -(f ? f[id] : f_const) - lap;
+      const double old_u = grid[id];
+      const double rhs = -f_plus_nl(f ? f[id] : f_const, nl, old_u) - lap;
       const double upd = __ddiv_rn(rhs, s.c);
       next[id] = upd;
-      acc[0] = fmax(acc[0], fabs(upd - grid[id]));
+      acc[0] = fmax(acc[0], fabs(upd - old_u));
     }
   }
   grid_reduce<1, true>(acc, slot, post);

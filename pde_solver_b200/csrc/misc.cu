@@ -18,9 +18,10 @@ struct PostAux {
 
 // ComputeResidualNorms (src/residual.cpp:153-723): 2D visits every node and
 // boundary nodes use their closure with alpha + beta/h on every Robin face
-// (:359,399); interior r = center*u + neighbours + f. 3D is interior only.
+// (:359,399); interior r = center*u + neighbours + (f + nonlinear(u)) (:449-487).
+// 3D is interior only and leaves the nonlinear terms out (:592-719).
 template <class Coef>
-__global__ void k_residual_norms(GridDev g, Coef cf, const double* __restrict__ f, double fc,
+__global__ void k_residual_norms(GridDev g, Coef cf, const double* __restrict__ f, double fc, NonlinDev nl,
                                  const double* __restrict__ u, RedSlot s_sum, RedSlot s_max, Ctl* out) {
   double acc[1] = {0.0}, mx[1] = {0.0};
   for (long long t = gtid(); t < g.n; t += gstride()) {
@@ -51,8 +52,9 @@ __global__ void k_residual_norms(GridDev g, Coef cf, const double* __restrict__ 
     } else {
       const Stencil<double> s = cf.template at<double>(g, t);
       const double zp = g.dim == 3 ? u[t + g.sxy] : 0.0, zm = g.dim == 3 ? u[t - g.sxy] : 0.0;
+      const double fv = f ? f[t] : fc;
       r = s.c * u[t] + nb_sum<double>(s, u[t + 1], u[t - 1], u[t + g.nx], u[t - g.nx], zp, zm, g.dim) +
-          (f ? f[t] : fc);
+          (g.dim == 2 ? f_plus_nl(fv, nl, u[t]) : fv);
     }
     acc[0] += r * r;
     mx[0] = fmax(mx[0], fabs(r));
@@ -64,7 +66,7 @@ __global__ void k_residual_norms(GridDev g, Coef cf, const double* __restrict__ 
 pdeb200_status residual_norms_dev(Context* ctx, DevProblem& P, const double* d_grid, double* l2, double* linf) {
   with_coef(P, [&](const auto& cf) {
     using Coef = std::decay_t<decltype(cf)>;
-    k_residual_norms<Coef><<<vec_blocks(P.g.n, ctx), 256, 0, ctx->stream>>>(P.g, cf, P.f, P.f_const, d_grid,
+    k_residual_norms<Coef><<<vec_blocks(P.g.n, ctx), 256, 0, ctx->stream>>>(P.g, cf, P.f, P.f_const, P.nl, d_grid,
                                                                             ctx->slot(0), ctx->slot(1), ctx->d_ctl);
   });
   ctx->count();
@@ -77,11 +79,11 @@ pdeb200_status residual_norms_dev(Context* ctx, DevProblem& P, const double* d_g
 // -------------------------------------------------------------- time series
 
 // One forward-Euler step of SolvePDETimeSeries (solver.cpp:1282-1319):
-// interior next = u + dt * SafeDivClamped(-(L u + f), ut, 0); boundary nodes
-// copied (their closures at t+dt follow in k_fill_boundary).
+// interior next = u + dt * SafeDivClamped(-(L u + f + nonlinear(u)), ut, 0);
+// boundary nodes copied (their closures at t+dt follow in k_fill_boundary).
 template <class Coef>
 __global__ void __launch_bounds__(kBx* kBy) k_fe_step(GridDev g, Coef cf, const double* __restrict__ f, double fc,
-                                                      double ut, double dt, const double* __restrict__ u,
+                                                      NonlinDev nl, double ut, double dt, const double* __restrict__ u,
                                                       double* __restrict__ next) {
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
@@ -98,7 +100,8 @@ __global__ void __launch_bounds__(kBx* kBy) k_fe_step(GridDev g, Coef cf, const 
     const Stencil<double> s = cf.template at<double>(g, id);
     const double zp = g.dim == 3 ? u[id + g.sxy] : 0.0, zm = g.dim == 3 ? u[id - g.sxy] : 0.0;
     const double opv = s.c * u[id] + nb_sum<double>(s, u[id + 1], u[id - 1], u[id + g.nx], u[id - g.nx], zp, zm, g.dim);
-    const double rhs = opv + (f ? f[id] : fc);
+    // (op + f) + nonlinear, the reference's left-to-right sum (solver.cpp:1300-1302)
+    const double rhs = nl.n ? __dadd_rn(opv + (f ? f[id] : fc), nl_eval(nl, u[id])) : opv + (f ? f[id] : fc);
     double u_t = 0.0;
     if (!(fabs(ut) < 1e-12)) {
       u_t = -rhs / ut;
@@ -145,7 +148,8 @@ pdeb200_status time_series_dev(Context* ctx, DevProblem& P, const pdeb200_time_o
     if (frame + 1 >= frames) break;
     with_coef(P, [&](const auto& cf) {
       using Coef = std::decay_t<decltype(cf)>;
-      k_fe_step<Coef><<<grid, block, 0, ctx->stream>>>(g, cf, P.f, P.f_const, P.ut, t->dt, buf[cur], buf[cur ^ 1]);
+      k_fe_step<Coef><<<grid, block, 0, ctx->stream>>>(g, cf, P.f, P.f_const, P.nl, P.ut, t->dt, buf[cur],
+                                                       buf[cur ^ 1]);
     });
     ctx->count();
     cur ^= 1;

@@ -10,17 +10,21 @@
 // array that every GPU loading the library holds until the process exits.
 //
 // Limits and sharing: the array holds kNoAllocMaxNodes nodes of the second
-// field (grids beyond that are rejected with PDEB200_ERR_UNSUPPORTED), and
-// every call uses the same array. Calls that overlap on the GPU (two host
-// threads, or two streams, at once) race on it and corrupt each other; the
-// caller serialises them. Each call clears what must start at zero (the
-// control block, the reduction tickets, the second field).
+// field and kNoAllocMaxBlocks reduction slots, one per x-y block of 32 x 8
+// columns, so a grid must have at most 1048576 nodes and
+// ceil(nx/32)*ceil(ny/8) <= 8192 (a long, thin 2D grid can reach the second
+// limit first); larger grids are rejected with PDEB200_ERR_UNSUPPORTED. Every
+// call uses the same array. Calls that overlap on the GPU (two host threads,
+// or two streams, at once) race on it and corrupt each other; the caller
+// serialises them. Each call clears what must start at zero (the control
+// block, the reduction tickets, the second field).
 //
-// Set-up: the first call on a device looks up the array's device address
-// with cudaGetSymbolAddress while that device is current, and caches it.
-// That first call should come before any stream capture on the device.
+// Set-up: every call looks up the array's device address with
+// cudaGetSymbolAddress while the device is current (the first call on a
+// device also loads the module there, so it should come before any stream
+// capture on that device). The address is not cached, so a device reset
+// between calls is harmless.
 #include <cstring>
-#include <mutex>
 
 #include "host.h"
 
@@ -47,8 +51,6 @@ constexpr size_t kNoAllocBytes = (sizeof(NoAllocLayout) + 255) / 256 * 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocDevices] = {nullptr};
 
 struct PostDeltaNA {
   Ctl* c;
@@ -65,18 +67,17 @@ struct PostDeltaNA {
   }
 };
 
+// Looked up on every call (with `device` current), not cached: after a
+// cudaDeviceReset the module is loaded again and the array may move.
 NoAllocLayout* scratch_for(int device) {
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw StatusFailure{PDEB200_ERR_CUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e)};
-    }
-    g_noalloc_ptr[device] = p;
+  (void)device;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw StatusFailure{PDEB200_ERR_CUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e)};
   }
-  return static_cast<NoAllocLayout*>(g_noalloc_ptr[device]);
+  return static_cast<NoAllocLayout*>(p);
 }
 
 int launch_blocks(const dim3& g) { return (int)((long long)g.x * g.y * g.z); }
@@ -116,7 +117,8 @@ static pdeb200_status jacobi_noalloc(const pdeb200_problem* p, int32_t max_iter_
   const int max_iter = max_iter_in > 1 ? max_iter_in : 1;
   const dim3 grid = stencil_grid_auto(g), block = stencil_block();
   if (launch_blocks(grid) > kNoAllocMaxBlocks)
-    throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "x-y plane too wide for the reduction scratch of pdeb200_jacobi_noalloc"};
+    throw StatusFailure{PDEB200_ERR_UNSUPPORTED,
+                        "x-y plane too wide for pdeb200_jacobi_noalloc: ceil(nx/32)*ceil(ny/8) must be at most 8192"};
   if (P.coef_kind == kConst && std::fabs(P.cc.c) < 1e-12)
     throw StatusFailure{PDEB200_ERR_DEGENERATE, "degenerate PDE center coefficient"};
 
@@ -143,7 +145,7 @@ static pdeb200_status jacobi_noalloc(const pdeb200_problem* p, int32_t max_iter_
       double* dst = buf[(t + 1) & 1];
       with_coef(P, [&](const auto& cf) {
         using Coef = std::decay_t<decltype(cf)>;
-        k_jacobi<Coef, PostDeltaNA><<<grid, block, 0, stream>>>(g, cf, P.f, P.f_const, src, dst, slot,
+        k_jacobi<Coef, PostDeltaNA><<<grid, block, 0, stream>>>(g, cf, P.f, P.f_const, P.nl, src, dst, slot,
                                                                  PostDeltaNA{&S->ctl}, &S->ctl, &S->degenerate);
       });
       k_fill_boundary<<<fb, 256, 0, stream>>>(g, dst, &S->ctl, 1);

@@ -1,4 +1,7 @@
-// Drivers not yet specialised for the B200 path report UNSUPPORTED.
+// Full-grid right side of the reference's Krylov path (BuildRhs2D,
+// src/backends/cpu/solver.cpp:167-232: Dirichlet values on boundary rows,
+// -f inside) and the one-shot operator apply behind pdeb200_apply
+// (LinearOperator2D::Apply, src/backends/cpu/cpu_utils.cpp:324-513).
 #include "host.h"
 #include "solvers.cuh"
 

@@ -65,12 +65,13 @@ __device__ void block_fill_boundary(const GridDev& g, double* u, bool dirichlet_
   }
 }
 
-// One node of the reference sweep: rhs = -(f) - (lap); upd = rhs/center;
-// SOR: (1-omega)*old + omega*upd (relaxation.cpp:266-276, solver.cpp:955-962).
+// One node of the reference sweep: rhs = -(f + nonlinear(old)) - (lap);
+// upd = rhs/center; SOR: (1-omega)*old + omega*upd (relaxation.cpp:217-276,
+// solver.cpp:884-962).
 template <class Coef>
 __device__ __forceinline__ double lex_update(const GridDev& g, const Coef& cf, const double* __restrict__ f,
-                                             double fc, double* u, int i, int j, int k, double omega, double* delta,
-                                             int* degenerate) {
+                                             double fc, const NonlinDev& nl, double* u, int i, int j, int k,
+                                             double omega, double* delta, int* degenerate) {
   const long long id = ((long long)k * g.ny + j) * g.nx + i;
   const Stencil<double> s = cf.template at<double>(g, id);
   if (fabs(s.c) < 1e-12) {
@@ -80,7 +81,7 @@ __device__ __forceinline__ double lex_update(const GridDev& g, const Coef& cf, c
   const double old_u = u[id];
   const double zp = g.dim == 3 ? u[id + g.sxy] : 0.0, zm = g.dim == 3 ? u[id - g.sxy] : 0.0;
   const double lap = nb_sum<double>(s, u[id + 1], u[id - 1], u[id + g.nx], u[id - g.nx], zp, zm, g.dim);
-  const double rhs = -(f ? f[id] : fc) - lap;
+  const double rhs = -f_plus_nl(f ? f[id] : fc, nl, old_u) - lap;
   const double upd = __ddiv_rn(rhs, s.c);
   const double updated = (1.0 - omega) * old_u + omega * upd;
   u[id] = updated;
@@ -121,7 +122,7 @@ __device__ __forceinline__ int hyper_hi(const GridDev& g) {
 // (solver.cpp:769-981; the initial closures are applied by the host).
 template <class Coef>
 __global__ void __launch_bounds__(1024) k_gs_lex_block(GridDev g, Coef cf, const double* __restrict__ f, double fc,
-                                                       double* u, double omega, double tol, int max_iter,
+                                                       NonlinDev nl, double* u, double omega, double tol, int max_iter,
                                                        unsigned long long budget_ns, Ctl* ctl) {
   __shared__ double red[32];
   __shared__ int s_stop;
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(1024) k_gs_lex_block(GridDev g, Coef cf, const
     const int dlo = hyper_lo(g), dhi = hyper_hi(g);
     for (int d = dlo; d <= dhi; ++d) {
       for_hyperplane(g, d, tid, blockDim.x,
-                     [&](int i, int j, int k) { lex_update(g, cf, f, fc, u, i, j, k, omega, &delta, &degen); });
+                     [&](int i, int j, int k) { lex_update(g, cf, f, fc, nl, u, i, j, k, omega, &delta, &degen); });
       __syncthreads();
     }
     if (degen) s_degen = 1;
@@ -188,13 +189,13 @@ __global__ void __launch_bounds__(1024) k_gs_lex_block(GridDev g, Coef cf, const
 // Multi-block form: one launch per hyperplane; max|du| through an atomic max
 // on the (non-negative) double's bit pattern in ctl->aux[0].
 template <class Coef>
-__global__ void k_gs_lex_plane(GridDev g, Coef cf, const double* __restrict__ f, double fc, double* u, double omega,
-                               int d, Ctl* ctl, int* degenerate) {
+__global__ void k_gs_lex_plane(GridDev g, Coef cf, const double* __restrict__ f, double fc, NonlinDev nl, double* u,
+                               double omega, int d, Ctl* ctl, int* degenerate) {
   if (ctl_stopped(ctl)) return;
   double delta = 0.0;
   int degen = 0;
   for_hyperplane(g, d, gtid(), gstride(),
-                 [&](int i, int j, int k) { lex_update(g, cf, f, fc, u, i, j, k, omega, &delta, &degen); });
+                 [&](int i, int j, int k) { lex_update(g, cf, f, fc, nl, u, i, j, k, omega, &delta, &degen); });
   if (degen) *degenerate = 1;
   for (int off = 16; off > 0; off >>= 1) delta = fmax(delta, __shfl_down_sync(0xffffffffu, delta, off));
   if ((threadIdx.x & 31) == 0 && delta > 0.0)
@@ -233,7 +234,8 @@ pdeb200_status gauss_seidel(Context* ctx, DevProblem& P, const Coef& cf, const p
     throw StatusFailure{PDEB200_ERR_UNSUPPORTED, "red-black ordering is offered through the MG forms"};
   if (interior <= (1LL << 18)) {
     const unsigned long long budget = 60ULL * 1000000000ULL;  // device-time guard: 60 s
-    k_gs_lex_block<Coef><<<1, 1024, 0, ctx->stream>>>(g, cf, P.f, P.f_const, d_out, omega, o->tol, max_iter, budget,
+    k_gs_lex_block<Coef><<<1, 1024, 0, ctx->stream>>>(g, cf, P.f, P.f_const, P.nl, d_out, omega, o->tol, max_iter,
+                                                      budget,
                                                       ctx->d_ctl);
     ctx->count();
     const Ctl& c = ctl_poll(ctx);
@@ -252,7 +254,7 @@ pdeb200_status gauss_seidel(Context* ctx, DevProblem& P, const Coef& cf, const p
     if (g.dim == 2) fill_boundary(ctx, g, d_out, ctx->d_ctl, false);
     for (int d = dlo; d <= dhi; ++d) {
       k_gs_lex_plane<Coef><<<vec_blocks((long long)(g.ny) * g.nz, ctx), 256, 0, ctx->stream>>>(
-          g, cf, P.f, P.f_const, d_out, omega, d, ctx->d_ctl, degen.as<int>());
+          g, cf, P.f, P.f_const, P.nl, d_out, omega, d, ctx->d_ctl, degen.as<int>());
     }
     ctx->count(dhi - dlo + 1);
     if (g.dim == 3) fill_boundary(ctx, g, d_out, ctx->d_ctl);

@@ -337,6 +337,18 @@ void describe_problem(Context* ctx, const pdeb200_problem* p, DevProblem* P) {
   P->coef_kind = p->coef_kind;
   P->f_const = p->f_const;
   P->device_inputs = p->mem_space == PDEB200_MEM_DEVICE;
+  if (p->n_nonlinear < 0 || p->n_nonlinear > PDEB200_MAX_NONLINEAR || (p->n_nonlinear > 0 && !p->nonlinear))
+    throw StatusFailure{PDEB200_ERR_INVALID, "nonlinear terms: at most 8, with a term array"};
+  P->nl = NonlinDev{};
+  P->nl.n = p->n_nonlinear;
+  for (int t = 0; t < p->n_nonlinear; ++t) {
+    const pdeb200_nonlinear_term& nt = p->nonlinear[t];
+    if (nt.kind < PDEB200_NL_POWER || nt.kind > PDEB200_NL_ABS)
+      throw StatusFailure{PDEB200_ERR_INVALID, "unknown nonlinear term kind"};
+    P->nl.kind[t] = nt.kind;
+    P->nl.power[t] = nt.power;
+    P->nl.coeff[t] = nt.coeff;
+  }
   build_faces(ctx, p, g.nx, g.ny, g.nz, P->dx, P->dy, P->dz, 1, &g, &P->owned);
   switch (p->coef_kind) {
     case PDEB200_COEF_CONST:

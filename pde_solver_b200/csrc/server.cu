@@ -46,6 +46,7 @@ struct SReq {
   pdeb200_problem prob{};
   std::vector<double> f, k, nodal, u0;
   std::vector<double> fa[6][4];
+  std::vector<pdeb200_nonlinear_term> nl;
   std::vector<double> pu, pv, pw, pp;
   int steps = 0;
   double tol = 1e-10, t_start = 0.0, dt = 0.0;
@@ -313,6 +314,14 @@ static void copy_problem(SReq* r, const pdeb200_problem* p) {
     r->prob.face[f].alpha_arr = grab(p->face[f].alpha_arr, cnt, &r->fa[f][1]);
     r->prob.face[f].beta_arr = grab(p->face[f].beta_arr, cnt, &r->fa[f][2]);
     r->prob.face[f].gamma_arr = grab(p->face[f].gamma_arr, cnt, &r->fa[f][3]);
+  }
+  // nonlinear terms are a host array in every memory space: copied
+  if (p->n_nonlinear > 0 && p->nonlinear) {
+    r->nl.assign(p->nonlinear, p->nonlinear + p->n_nonlinear);
+    r->prob.nonlinear = r->nl.data();
+  } else {
+    r->prob.n_nonlinear = 0;
+    r->prob.nonlinear = nullptr;
   }
 }
 

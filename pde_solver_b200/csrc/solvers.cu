@@ -34,7 +34,7 @@ pdeb200_status jacobi(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
   auto iterate = [&](int t) {
     double* src = buf[t & 1];
     double* dst = buf[(t + 1) & 1];
-    k_jacobi<Coef, PostDelta><<<grid, block, 0, ctx->stream>>>(g, cf, P.f, P.f_const, src, dst, ctx->slot(),
+    k_jacobi<Coef, PostDelta><<<grid, block, 0, ctx->stream>>>(g, cf, P.f, P.f_const, P.nl, src, dst, ctx->slot(),
                                                                PostDelta{ctx->d_ctl}, ctx->d_ctl, degen.as<int>());
     fill_boundary(ctx, g, dst, ctx->d_ctl);
     ctx->count();
@@ -199,9 +199,15 @@ pdeb200_status solve_dispatch(Context* ctx, DevProblem& P, const pdeb200_problem
       if (P.g.face[f].active && P.g.face[f].kind != kDirichlet) return false;
     return true;
   }();
-  if (P.coef_kind == kConst && std::fabs(P.cc.c) < 1e-12 &&
-      (o->method == PDEB200_JACOBI || o->method == PDEB200_GAUSS_SEIDEL || o->method == PDEB200_SOR))
+  const bool relaxation = o->method == PDEB200_JACOBI || o->method == PDEB200_GAUSS_SEIDEL || o->method == PDEB200_SOR;
+  if (P.coef_kind == kConst && std::fabs(P.cc.c) < 1e-12 && relaxation)
     throw StatusFailure{PDEB200_ERR_DEGENERATE, "degenerate PDE center coefficient"};
+  // pointwise nonlinear terms: relaxation only (src/backends/cpu/solver.cpp:502,550)
+  if (P.nl.n > 0 && !relaxation)
+    throw StatusFailure{PDEB200_ERR_UNSUPPORTED, o->method == PDEB200_CG || o->method == PDEB200_BICGSTAB ||
+                                                         o->method == PDEB200_GMRES
+                                                     ? "Krylov solvers require linear PDEs"
+                                                     : "Multigrid requires linear PDEs"};
   with_coef(P, [&](const auto& cf) {
     switch (o->method) {
       case PDEB200_JACOBI:

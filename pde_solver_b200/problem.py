@@ -68,6 +68,9 @@ class GridProblem:
     f: np.ndarray | None = None
     u0: np.ndarray | None = None
     faces: list = field(default_factory=lambda: [FaceBC() for _ in range(6)])
+    # pointwise nonlinear terms (NonlinearTerm, include/pde_types.h:96-100):
+    # (kind, coeff, power) with kind one of abi.NL_*
+    nonlinear: list = field(default_factory=list)
     mem_space: int = abi.MEM_HOST
     # device pointers (MEM_DEVICE): ints
     k_dev: int = 0
@@ -136,6 +139,13 @@ class GridProblem:
                 arr = self._contig(getattr(fc, name))
                 self._keep.append(arr)
                 setattr(cf, name, _dptr(arr))
+        if self.nonlinear:
+            terms = (abi.NonlinearTerm * len(self.nonlinear))()
+            for t, (kind, coeff, power) in zip(terms, self.nonlinear):
+                t.kind, t.coeff, t.power = int(kind), float(coeff), int(power)
+            self._keep.append(terms)
+            p.n_nonlinear = len(self.nonlinear)
+            p.nonlinear = C.cast(terms, C.POINTER(abi.NonlinearTerm))
         return p
 
 

@@ -35,6 +35,7 @@ namespace {
 struct Materialised {
   pdeb200_problem prob{};
   std::vector<double> f, nodal, u0;
+  std::vector<pdeb200_nonlinear_term> nonlinear;
   std::vector<double> face_arr[6][4];
   std::string error;
 };
@@ -48,8 +49,12 @@ bool Unsupported(const SolveInput& in, std::string* why) {
     *why = "B200 backend requires CPU fallback: implicit domain shape unsupported";
     return true;
   }
-  if (!in.integrals.empty() || !in.nonlinear.empty() || !in.nonlinear_derivatives.empty()) {
-    *why = "B200 backend requires CPU fallback: integral or nonlinear terms unsupported";
+  if (!in.integrals.empty() || !in.nonlinear_derivatives.empty()) {
+    *why = "B200 backend requires CPU fallback: integral or nonlinear derivative terms unsupported";
+    return true;
+  }
+  if (in.nonlinear.size() > PDEB200_MAX_NONLINEAR) {
+    *why = "B200 backend requires CPU fallback: more than 8 nonlinear terms";
     return true;
   }
   if (HasMixedDerivatives(in.pde) || HasHigherOrderDerivatives(in.pde)) {
@@ -175,6 +180,11 @@ bool Materialise(const SolveInput& in, Materialised* m, int device) {
     F.beta_arr = m->face_arr[f][2].data();
     F.gamma_arr = m->face_arr[f][3].data();
   }
+  // pointwise nonlinear terms (NonlinearTerm, include/pde_types.h:96-100), same kind order
+  for (const NonlinearTerm& t : in.nonlinear)
+    m->nonlinear.push_back(pdeb200_nonlinear_term{static_cast<int32_t>(t.kind), t.power, t.coeff});
+  p.n_nonlinear = (int32_t)m->nonlinear.size();
+  p.nonlinear = m->nonlinear.empty() ? nullptr : m->nonlinear.data();
   if (!in.initial_grid.empty()) {
     if ((long long)in.initial_grid.size() != n) {
       m->error = "initial grid size mismatch";
@@ -236,6 +246,10 @@ SolveOutput SolvePDECuda(const SolveInput& input) {
   FillOptions(input, &o);
   const bool krylov = input.solver.method == SolveMethod::CG || input.solver.method == SolveMethod::BiCGStab ||
                       input.solver.method == SolveMethod::GMRES;
+  // the reference's order: linearity before the CG symmetry check (src/backends/cpu/solver.cpp:502,550)
+  if (!input.nonlinear.empty() && krylov) return {"Krylov solvers require linear PDEs", {}};
+  if (!input.nonlinear.empty() && input.solver.method == SolveMethod::MultigridVcycle)
+    return {"Multigrid requires linear PDEs", {}};
   if (input.solver.method == SolveMethod::CG && (HasVariableCoefficients(input.pde) ||
                                                  std::abs(input.pde.c) > 1e-12 || std::abs(input.pde.d) > 1e-12))
     return {"CG requires symmetric operators with constant coefficients (no convection/mixed/higher-order terms)", {}};

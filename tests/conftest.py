@@ -25,7 +25,7 @@ def gpu_available() -> bool:
 def oracle_mod():
     from oracle import oracle as O
 
-    O.build(ref=os.path.exists("/root/reference/src"))
+    O.build(ref=O.have_reference_sources())
     return O
 
 

@@ -42,7 +42,49 @@ def solve_cases():
     p.faces = [FaceBC.dirichlet(0.5), FaceBC.dirichlet(0.0), FaceBC.dirichlet(1.0), FaceBC.dirichlet(0.0),
                FaceBC(), FaceBC()]
     out["bicgstab_2d"] = (p, default_options(method=abi.BICGSTAB, max_iter=3000, tol=1e-10), "x-y+1")
+    # Robin on the max faces (right, top, back): the closure there is
+    # u_N = (gamma - beta/h u_{N-1}) / (alpha - beta/h) (cpu_utils.cpp:671-673,853-855,893-895);
+    # alpha > 2 beta/h keeps |du_N/du_{N-1}| < 1, so the relaxation converges
+    p = GridProblem(23, 19, 1, a=-1.0, b=-1.0, c=0.3)
+    p.faces = [FaceBC.dirichlet(0.0), FaceBC.robin(2.0, 0.02, 0.3), FaceBC.dirichlet(0.5), FaceBC.robin(1.0, 0.02, 0.2),
+               FaceBC(), FaceBC()]
+    out["jacobi_maxrobin_2d"] = (p, default_options(method=abi.JACOBI, max_iter=40000, tol=1e-11), "x-y")
+    p = GridProblem(11, 10, 9, a=-1.0, b=-1.0, az=-1.0)
+    p.faces = [FaceBC.neumann(0.1), FaceBC.robin(2.0, 0.05, 0.2), FaceBC.dirichlet(0.0), FaceBC.robin(1.5, 0.03, 0.0),
+               FaceBC.dirichlet(0.25), FaceBC.robin(2.0, 0.05, -0.1)]
+    out["sor_maxrobin_3d"] = (p, default_options(method=abi.SOR, sor_omega=1.5, max_iter=40000, tol=1e-12), "1+x*z")
+    # pointwise nonlinear terms (EvalNonlinear, relaxation.cpp:27-45, solver.cpp:234-256)
+    p = GridProblem(25, 21, 1, a=-1.0, b=-1.0)
+    p.faces = faces_2d()
+    p.nonlinear = [(abi.NL_POWER, 0.5, 2)]
+    out["jacobi_nl_u2_2d"] = (p, default_options(method=abi.JACOBI, max_iter=40000, tol=1e-11), "x*y-1")
+    p = GridProblem(25, 21, 1, a=-1.0, b=-1.0, c=0.4)
+    p.faces = faces_2d()
+    p.nonlinear = [(abi.NL_SIN, 2.0, 2)]
+    out["sor_nl_sin_2d"] = (p, default_options(method=abi.SOR, sor_omega=1.6, max_iter=40000, tol=1e-12), "1+x")
+    p = GridProblem(11, 9, 10, a=-1.0, b=-1.0, az=-1.0)
+    p.faces = faces_3d()
+    p.nonlinear = [(abi.NL_EXP, 0.3, 2)]
+    out["gs_nl_exp_3d"] = (p, default_options(method=abi.GAUSS_SEIDEL, max_iter=40000, tol=1e-12), "x-z")
+    p = GridProblem(12, 11, 10, a=-1.0, b=-1.0, az=-1.0)
+    p.faces = faces_3d()
+    p.nonlinear = [(abi.NL_POWER, -0.4, 3), (abi.NL_COS, 0.5, 2), (abi.NL_ABS, 0.7, 2)]
+    out["jacobi_nl_mixed_3d"] = (p, default_options(method=abi.JACOBI, max_iter=40000, tol=1e-11), "y+1")
     return out
+
+
+def heat_nl_case():
+    """2D heat step with a pointwise nonlinear source (solver.cpp:1298-1302)."""
+    p, t0, dt, frames = heat_case()
+    p.nonlinear = [(abi.NL_POWER, 0.8, 2), (abi.NL_SIN, -0.5, 2)]
+    return p, t0, dt, frames
+
+
+def residual_nl_case():
+    """2D residual norms with nonlinear terms (residual.cpp:449-487)."""
+    p, grid = residual_case()
+    p.nonlinear = [(abi.NL_POWER, 0.25, 3), (abi.NL_EXP, 0.1, 2)]
+    return p, grid
 
 
 def heat_case():

@@ -39,6 +39,13 @@ def main():
     p, grid = cases.residual_case()
     l2, linf = oracle.ref_residual_norms(p, grid)
     out["residual_2d/norms"] = np.array([l2, linf])
+    p, t0, dt, frames = cases.heat_nl_case()
+    grid, fr = oracle.ref_time_series(p, t0, dt, frames, keep_frames=True)
+    out["heat_nl_2d/grid"] = grid
+    out["heat_nl_2d/frames"] = fr
+    p, grid = cases.residual_nl_case()
+    l2, linf = oracle.ref_residual_norms(p, grid)
+    out["residual_nl_2d/norms"] = np.array([l2, linf])
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_cases.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, len(out), "arrays")

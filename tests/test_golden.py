@@ -58,11 +58,18 @@ def test_restatement_projection_fixture(oracle_mod):
     assert rep.poisson_iterations == int(FIX["projection_2d/report"][0])
 
 
-def test_restatement_residual_fixture(oracle_mod):
-    p, grid = cases.residual_case()
+@pytest.mark.parametrize("case,key", [(cases.residual_case, "residual_2d"), (cases.residual_nl_case, "residual_nl_2d")])
+def test_restatement_residual_fixture(oracle_mod, case, key):
+    p, grid = case()
     l2, linf = oracle_mod.rs_residual_norms(p, grid)
-    assert l2 == pytest.approx(FIX["residual_2d/norms"][0], rel=1e-12)
-    assert linf == pytest.approx(FIX["residual_2d/norms"][1], rel=1e-12)
+    assert l2 == pytest.approx(FIX[f"{key}/norms"][0], rel=1e-12)
+    assert linf == pytest.approx(FIX[f"{key}/norms"][1], rel=1e-12)
+
+
+def test_restatement_heat_nonlinear_fixture(oracle_mod):
+    p, t0, dt, frames = cases.heat_nl_case()
+    got, fr = oracle_mod.rs_time_series(p, t0, dt, frames, keep_frames=True)
+    assert rel_l2(fr, FIX["heat_nl_2d/frames"]) <= 1e-12
 
 
 @pytest.mark.gpu
@@ -78,12 +85,13 @@ def test_cuda_path_matches_reference_fixture(lib, name):
 
 
 @pytest.mark.gpu
-def test_cuda_heat_matches_reference_fixture(lib):
+@pytest.mark.parametrize("case,key", [(cases.heat_case, "heat_2d"), (cases.heat_nl_case, "heat_nl_2d")])
+def test_cuda_heat_matches_reference_fixture(lib, case, key):
     from pde_solver_b200 import solver
 
-    p, t0, dt, frames = cases.heat_case()
+    p, t0, dt, frames = case()
     got, _ = solver.time_series(p, t0, dt, frames)
-    assert rel_l2(got, FIX["heat_2d/grid"]) <= 1e-12
+    assert rel_l2(got, FIX[f"{key}/grid"]) <= 1e-12
 
 
 @pytest.mark.gpu
@@ -93,15 +101,20 @@ def test_cuda_projection_matches_reference_fixture(lib):
     c = cases.projection_case()
     u, v, _, pr, rep = solver.project_velocity(c["u"], c["v"], c["w"], c["p"], c["nx"], c["ny"], c["nz"], c["dx"],
                                               c["dy"], c["dz"], c["dt"], c["max_iter"], c["tol"])
+    # the same CG in the same order: only FMA contraction and the reduction
+    # order differ, which moves the fields by about 1e-13
+    assert rep.poisson_iterations == int(FIX["projection_2d/report"][0])
     for a, key in ((u, "u"), (v, "v"), (pr, "p")):
-        assert rel_l2(a, FIX[f"projection_2d/{key}"]) <= 1e-8
+        d = rel_l2(a, FIX[f"projection_2d/{key}"])
+        assert d <= 1e-10, (key, d)
 
 
 @pytest.mark.gpu
-def test_cuda_residual_norms_match_reference_fixture(lib):
+@pytest.mark.parametrize("case,key", [(cases.residual_case, "residual_2d"), (cases.residual_nl_case, "residual_nl_2d")])
+def test_cuda_residual_norms_match_reference_fixture(lib, case, key):
     from pde_solver_b200 import solver
 
-    p, grid = cases.residual_case()
+    p, grid = case()
     l2, linf = solver.residual_norms(p, grid)
-    assert l2 == pytest.approx(FIX["residual_2d/norms"][0], rel=1e-12)
-    assert linf == pytest.approx(FIX["residual_2d/norms"][1], rel=1e-12)
+    assert l2 == pytest.approx(FIX[f"{key}/norms"][0], rel=1e-12)
+    assert linf == pytest.approx(FIX[f"{key}/norms"][1], rel=1e-12)

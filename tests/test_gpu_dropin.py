@@ -104,3 +104,53 @@ def test_time_series_through_shim(drop):
     assert st == 0, err
     cpu, cframes = drop.ref_time_series(p, 0.0, dt, 30, keep_frames=True)
     assert rel_l2(gframes, cframes) <= 1e-12
+
+
+def test_nonlinear_jacobi_through_solve_with_backend(drop):
+    # pointwise nonlinear terms reach the CUDA backend: the reference's capability
+    # row for CUDA advertises them (src/backend_capability_matrix.cpp:105)
+    p = GridProblem(33, 29, 1, a=-1.0, b=-1.0)
+    p.faces = [FaceBC.robin(1.0, 0.5, 0.2), FaceBC.dirichlet(0.0), FaceBC.neumann(0.3), FaceBC.dirichlet(1.0),
+               FaceBC(), FaceBC()]
+    p.nonlinear = [(abi.NL_POWER, 0.5, 2), (abi.NL_SIN, 1.0, 2)]
+    opt = default_options(method=abi.JACOBI, max_iter=40000, tol=1e-11)
+    st, gpu, _, sel, err = drop.dropin_solve(p, opt, 1, rhs_latex="x*y-1")
+    assert st == 0 and sel, err
+    st, cpu, _, _, err = drop.dropin_solve(p, opt, 0, rhs_latex="x*y-1")
+    assert st == 0, err
+    assert rel_l2(gpu, cpu) <= 1e-10
+
+
+def test_nonlinear_sor_3d_through_solve_pde_cuda(drop):
+    p = GridProblem(13, 11, 10, a=-1.0, b=-1.0, az=-1.0)
+    p.faces = [FaceBC.dirichlet(0.0), FaceBC.dirichlet(0.5), FaceBC.neumann(0.0), FaceBC.neumann(0.2),
+               FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(0.0)]
+    p.nonlinear = [(abi.NL_EXP, 0.3, 2)]
+    opt = default_options(method=abi.SOR, sor_omega=1.5, max_iter=40000, tol=1e-11)
+    st, gpu, err = drop.dropin_solve_cuda(p, opt, rhs_latex="x-z")
+    assert st == 0, err
+    st, cpu, _, _, err = drop.dropin_solve(p, opt, 0, rhs_latex="x-z")
+    assert st == 0, err
+    assert rel_l2(gpu, cpu) <= 1e-10
+
+
+def test_nonlinear_krylov_refused_with_reference_text(drop):
+    p = GridProblem(17, 17, 1, a=-1.0, b=-1.0)
+    p.nonlinear = [(abi.NL_POWER, 1.0, 2)]
+    st, _, err = drop.dropin_solve_cuda(p, default_options(method=abi.CG))
+    assert st != 0 and err == "Krylov solvers require linear PDEs"
+
+
+def test_nonlinear_time_series_through_shim(drop):
+    n = 33
+    p = GridProblem(n, n, 1, a=-1.0, b=-1.0, ut=1.0)
+    p.faces = [FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(0.0),
+               FaceBC(), FaceBC()]
+    x, y, _ = p.coords()
+    p.u0 = np.exp(-40 * ((x - 0.5) ** 2 + (y - 0.5) ** 2)).reshape(-1)
+    p.nonlinear = [(abi.NL_POWER, 0.8, 2), (abi.NL_SIN, -0.5, 2)]
+    dt = 0.9 * (1.0 / (n - 1)) ** 2 / 4
+    st, gpu, gframes, err = drop.dropin_time_series_cuda(p, 0.0, dt, 30)
+    assert st == 0, err
+    cpu, cframes = drop.ref_time_series(p, 0.0, dt, 30, keep_frames=True)
+    assert rel_l2(gframes, cframes) <= 1e-12

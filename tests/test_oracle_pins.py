@@ -208,3 +208,40 @@ def test_residual_norms(ref_oracle, dim):
     l2s, lis = ref_oracle.rs_residual_norms(prob, grid)
     assert l2s == pytest.approx(l2r, rel=1e-14)
     assert lis == pytest.approx(lir, rel=1e-14)
+
+
+NONLINEAR = [
+    ("u2", [(abi.NL_POWER, 0.5, 2)]),
+    ("sin", [(abi.NL_SIN, 2.0, 2)]),
+    ("exp", [(abi.NL_EXP, 0.3, 2)]),
+    ("cube_cos_abs", [(abi.NL_POWER, -0.4, 3), (abi.NL_COS, 0.5, 2), (abi.NL_ABS, 0.7, 2)]),
+]
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("method,omega", [(abi.JACOBI, 1.0), (abi.GAUSS_SEIDEL, 1.0), (abi.SOR, 1.5)])
+@pytest.mark.parametrize("name,terms", NONLINEAR)
+def test_relaxation_nonlinear_terms(ref_oracle, dim, method, omega, name, terms):
+    # EvalNonlinear at the node's old value inside every update
+    # (relaxation.cpp:27-45,217-218,476-477; solver.cpp:884-885)
+    dims = (21, 19, 1) if dim == 2 else (11, 10, 9)
+    prob = GridProblem(*dims, a=-1.0, b=-1.0, az=-1.0, c=0.3)
+    prob.faces = _mixed_faces_2d() if dim == 2 else _mixed_faces_3d()
+    prob.nonlinear = terms
+    opt = default_options(method=method, max_iter=40000, tol=1e-11, sor_omega=omega)
+    ref, rs, rep = _pair(ref_oracle, prob, opt, rhs_latex="x*y-1")
+    assert rel_l2(rs, ref) <= REL
+
+
+@pytest.mark.parametrize("method", [abi.CG, abi.BICGSTAB, abi.MG_VCYCLE])
+def test_nonlinear_terms_rejected_like_reference(ref_oracle, method):
+    prob = GridProblem(17, 17, 1, a=-1.0, b=-1.0)
+    prob.nonlinear = [(abi.NL_POWER, 1.0, 2)]
+    opt = default_options(method=method, max_iter=100, tol=1e-8)
+    # the reference's gate refuses first ("linear PDE required for this method",
+    # backend_capability_matrix.cpp:265-267); SolvePDE itself says "... require
+    # linear PDEs" (solver.cpp:502-504,550-552), the text the restatement gives
+    st, _, _, err = ref_oracle.ref_solve(prob, opt)
+    st2, _, rep = ref_oracle.rs_solve(prob, opt)
+    assert st != 0 and st2 == abi.ERR_UNSUPPORTED
+    assert "linear PDE" in err and "linear PDEs" in rep.message.decode()
