@@ -1107,94 +1107,72 @@ static void rbgs_color(const Grid* g, const double* b, double* x, int color) {
       }
 }
 
+/* Visit the nodes of face f in (k, j, i) order with i, j, k in scope. Within
+ * one face pass no two nodes share an inward neighbour, so the order of the
+ * visits does not change any value. */
+#define FACE_NODES(g, f, ...)                                                      \
+  do {                                                                             \
+    const int k_lo_ = (f) == BACK ? (g)->nz - 1 : 0, k_hi_ = (f) == FRONT ? 1 : (g)->nz; \
+    const int j_lo_ = (f) == TOP ? (g)->ny - 1 : 0, j_hi_ = (f) == BOTTOM ? 1 : (g)->ny; \
+    const int i_lo_ = (f) == RIGHT ? (g)->nx - 1 : 0, i_hi_ = (f) == LEFT ? 1 : (g)->nx; \
+    for (int k = k_lo_; k < k_hi_; ++k)                                            \
+      for (int j = j_lo_; j < j_hi_; ++j)                                          \
+        for (int i = i_lo_; i < i_hi_; ++i) __VA_ARGS__                            \
+  } while (0)
+
+/* The interior neighbour of face node (i, j, k) across face f. */
+static inline void inward(const Grid* g, int f, int i, int j, int k, int* ii, int* jj, int* kk) {
+  *ii = f == LEFT ? 1 : f == RIGHT ? g->nx - 2 : i;
+  *jj = f == BOTTOM ? 1 : f == TOP ? g->ny - 2 : j;
+  *kk = f == FRONT ? 1 : f == BACK ? g->nz - 2 : k;
+}
+
 /* Homogeneous closure extension of a correction field: boundary nodes take
  * c1 * (inward neighbour) in the reference's phase order (x, y, z faces),
  * Dirichlet nodes 0. Ext is the map the folded system eliminates, so
  * interpolating Ext(x_c) carries Neumann/Robin corrections to the faces. */
 static void ext_apply(const Grid* g, double* x) {
-  const int nx = g->nx, ny = g->ny, nz = g->nz;
   double c0, c1;
   for (int f = LEFT; f <= BACK; ++f) {
     if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
-                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
-          if (on) x[ID(g, i, j, k)] = 0.0;
-        }
+    FACE_NODES(g, f, x[ID(g, i, j, k)] = 0.0;);
   }
   for (int f = LEFT; f <= BACK; ++f) {
     if (!face_active(g, f) || face_kind(g, f) == PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          int on = 0, ii = i, jj = j, kk = k;
-          if (f == LEFT && i == 0) { on = 1; ii = 1; }
-          if (f == RIGHT && i == nx - 1) { on = 1; ii = nx - 2; }
-          if (f == BOTTOM && j == 0) { on = 1; jj = 1; }
-          if (f == TOP && j == ny - 1) { on = 1; jj = ny - 2; }
-          if (f == FRONT && k == 0) { on = 1; kk = 1; }
-          if (f == BACK && k == nz - 1) { on = 1; kk = nz - 2; }
-          if (!on) continue;
-          face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
-          x[ID(g, i, j, k)] = c1 * x[ID(g, ii, jj, kk)];
-        }
+    FACE_NODES(g, f, {
+      int ii, jj, kk;
+      inward(g, f, i, j, k, &ii, &jj, &kk);
+      face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
+      x[ID(g, i, j, k)] = c1 * x[ID(g, ii, jj, kk)];
+    });
   }
   for (int f = LEFT; f <= BACK; ++f) {
     if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
-                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
-          if (on) x[ID(g, i, j, k)] = 0.0;
-        }
+    FACE_NODES(g, f, x[ID(g, i, j, k)] = 0.0;);
   }
 }
 
 /* Transpose of ext_apply: Dirichlet nodes zeroed, then the Neumann/Robin
  * phases in reverse (z, y, x): y[inward] += c1*y[b], y[b] = 0. */
 static void ext_transpose(const Grid* g, double* y) {
-  const int nx = g->nx, ny = g->ny, nz = g->nz;
   double c0, c1;
   for (int f = LEFT; f <= BACK; ++f) {
     if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
-                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
-          if (on) y[ID(g, i, j, k)] = 0.0;
-        }
+    FACE_NODES(g, f, y[ID(g, i, j, k)] = 0.0;);
   }
   for (int f = BACK; f >= LEFT; --f) {
     if (!face_active(g, f) || face_kind(g, f) == PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          int on = 0, ii = i, jj = j, kk = k;
-          if (f == LEFT && i == 0) { on = 1; ii = 1; }
-          if (f == RIGHT && i == nx - 1) { on = 1; ii = nx - 2; }
-          if (f == BOTTOM && j == 0) { on = 1; jj = 1; }
-          if (f == TOP && j == ny - 1) { on = 1; jj = ny - 2; }
-          if (f == FRONT && k == 0) { on = 1; kk = 1; }
-          if (f == BACK && k == nz - 1) { on = 1; kk = nz - 2; }
-          if (!on) continue;
-          face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
-          y[ID(g, ii, jj, kk)] += c1 * y[ID(g, i, j, k)];
-          y[ID(g, i, j, k)] = 0.0;
-        }
+    FACE_NODES(g, f, {
+      int ii, jj, kk;
+      inward(g, f, i, j, k, &ii, &jj, &kk);
+      face_c01(g, f, flocal(g, f, i, j, k), &c0, &c1);
+      y[ID(g, ii, jj, kk)] += c1 * y[ID(g, i, j, k)];
+      y[ID(g, i, j, k)] = 0.0;
+    });
   }
   for (int f = LEFT; f <= BACK; ++f) {
     if (!face_active(g, f) || face_kind(g, f) != PDEB200_BC_DIRICHLET) continue;
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          const int on = (f == LEFT && i == 0) || (f == RIGHT && i == nx - 1) || (f == BOTTOM && j == 0) ||
-                         (f == TOP && j == ny - 1) || (f == FRONT && k == 0) || (f == BACK && k == nz - 1);
-          if (on) y[ID(g, i, j, k)] = 0.0;
-        }
+    FACE_NODES(g, f, y[ID(g, i, j, k)] = 0.0;);
   }
 }
 
@@ -1218,6 +1196,7 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   }
   /* r = b - A x */
   folded_apply(g, x, lv[l].r);
+#pragma omp parallel for schedule(static)
   for (long q = 0; q < g->n; ++q) lv[l].r[q] = b[q] - lv[l].r[q];
   /* full weighting r -> coarse b (tensor [1/4,1/2,1/4] for odd n, the scaled
    * transpose of the interpolation in general) at every coarse node, then the
@@ -1229,6 +1208,7 @@ static void mg_vcycle_folded(Level* lv, int L, int l, int pre, int post, int coa
   const int all = g_mg_boundary_transfer;
   const int kc0 = c->dim == 3 ? (all ? 0 : 1) : 0, kc1 = c->dim == 3 ? (all ? c->nz : c->nz - 1) : 1;
   const int ic0 = all ? 0 : 1, ic1 = all ? c->nx : c->nx - 1, jc0 = all ? 0 : 1, jc1 = all ? c->ny : c->ny - 1;
+#pragma omp parallel for collapse(2) schedule(static)
   for (int K = kc0; K < kc1; ++K)
     for (int J = jc0; J < jc1; ++J)
       for (int I = ic0; I < ic1; ++I) {
@@ -1323,6 +1303,7 @@ static int mg_pcg(const Grid* g, const pdeb200_options* o, double* x, pdeb200_re
       break;
     }
     const double alpha = rz / pq;
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < n; ++i) {
       x[i] += alpha * p[i];
       r[i] -= alpha * q[i];
@@ -1336,6 +1317,7 @@ static int mg_pcg(const Grid* g, const pdeb200_options* o, double* x, pdeb200_re
     PRECOND(z);
     const double rz_new = dot(r, z, n);
     const double beta = rz_new / rz;
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     rz = rz_new;
   }
