@@ -14,6 +14,13 @@ HBM (device pointers); `e2e` goes through the same C-ABI call with pinned host
 buffers, so every step includes the H2D copy of k and f and the D2H copy of the
 solution. Multi-GPU runs are independent replicas (no collective on the data
 path); each rank solves its own copy and the time is the max over ranks.
+
+CPU sides: `cpu_baseline` is two whole converged solves of the same input by
+the oracle port (oracle/restate.c) on all host cores; `--impl reference` times
+W + K whole converged solves the same way; `forms.reference_code` times the
+reference's own CPU code (oracle/_ref) where it has the method (2D CG and
+Jacobi at 129^2, 2D projection at 256^2) beside the GPU. `summary`, last in
+the line, repeats the forms' headline figures.
 """
 from __future__ import annotations
 
@@ -135,10 +142,9 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ CPU side
 
-def cpu_sample(prob, gpu_iters):
-    """Oracle port of the same MG-PCG on the host cores (OpenMP, all threads):
-    setup + 1 iteration and setup + 3 iterations on the same 257^3 input give
-    the per-iteration cost; a solve is setup + iterations-to-converge."""
+def cpu_solve_times(prob, count):
+    """Wall times of `count` whole converged solves of `prob` by the oracle port
+    of the same MG-PCG (oracle/restate.c) on all host cores."""
     from oracle import oracle
     from pde_solver_b200 import abi
     from pde_solver_b200.problem import default_options
@@ -146,19 +152,93 @@ def cpu_sample(prob, gpu_iters):
     cores = os.cpu_count() or 1
     oracle.build(ref=False)
     oracle.restate().rs_set_threads(cores)
-    times = {}
-    for its in (1, 3):
-        o = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=its)
+    o = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400)
+    times, iters = [], None
+    for _ in range(count):
         t0 = time.perf_counter()
-        oracle.rs_solve(prob, o)
-        times[its] = time.perf_counter() - t0
-    t_iter = max((times[3] - times[1]) / 2.0, 1e-9)
-    t_setup = max(times[1] - t_iter, 0.0)
-    t_solve = t_setup + gpu_iters * t_iter
-    return {"value": 1.0 / t_solve, "unit": UNIT, "cores": cores, "kind": "port",
+        st, _, rep = oracle.rs_solve(prob, o)
+        times.append(time.perf_counter() - t0)
+        if st != abi.OK:
+            raise RuntimeError(f"oracle solve failed: {st}")
+        iters = rep.iterations
+    return times, iters, cores
+
+
+def cpu_sample(prob, count=2):
+    """CPU baseline beside the GPU line: `count` whole converged solves of the
+    same input by the oracle port (the reference's CPU path has no 3D
+    divergence-form MG-PCG), median wall time."""
+    times, iters, cores = cpu_solve_times(prob, count)
+    t = statistics.median(times)
+    return {"value": 1.0 / t, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": (f"oracle/restate.c MG-PCG on the same {prob.nx}^3 input, OpenMP {cores} threads: "
-                       f"setup+1 and setup+3 iterations timed ({times[1]:.2f}s, {times[3]:.2f}s), "
-                       f"solve = setup + {gpu_iters} iterations = {t_solve:.2f}s")}
+                       f"{count} whole converged solves ({iters} iterations each), median "
+                       f"{t:.2f}s (all: {', '.join(f'{v:.2f}' for v in times)} s)")}
+
+
+def reference_code_paths(lib, abi, device):
+    """Configurations where the reference's own CPU code exists, timed beside
+    the GPU: 2D Poisson 129^2 with the MMS right side by CG (CgSolve) and by
+    Jacobi (SolveJacobi2D) to the reference's own stopping rules, and the 2D
+    pressure projection of a 256^2 N(0,1) velocity field (ProjectVelocity2D,
+    CG to 1e-10 relative). CPU: oracle/_ref (the reference compiled from its
+    sources), one whole call each, all host cores. GPU: the same call through
+    the C ABI with host buffers (copies included), median of 5 after one warm-up."""
+    from oracle import oracle
+    from pde_solver_b200 import solver, synthetic
+    from pde_solver_b200.problem import default_options
+
+    if not oracle.have_reference():
+        return {"unavailable": "oracle/_ref/libpderef.so not built"}
+    cores = os.cpu_count() or 1
+    oracle.reference().pderef_set_threads(cores)
+    out = {"cores": cores, "kind": "reference"}
+    for name, method, max_iter, tol in (("config1_cg_129", abi.CG, 8000, 1e-10),
+                                        ("config1_jacobi_129", abi.JACOBI, 200000, 1e-10)):
+        p = synthetic.poisson_mms_2d(129)
+        p.f = None
+        opt = default_options(method=method, max_iter=max_iter, tol=tol, device=device.index or 0)
+        t0 = time.perf_counter()
+        st, ref, _, err = oracle.ref_solve(p, opt, rhs_latex=synthetic.MMS_RHS_LATEX)
+        cpu_s = time.perf_counter() - t0
+        p.f = oracle.ref_materialize(synthetic.MMS_RHS_LATEX, p)
+        got, rep = solver.solve(p, opt)
+        ts = []
+        for _ in range(5):
+            torch_sync()
+            t0 = time.perf_counter()
+            got, rep = solver.solve(p, opt)
+            ts.append(time.perf_counter() - t0)
+        gpu_s = statistics.median(ts)
+        d = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        out[name] = {"cpu_ms": 1e3 * cpu_s, "gpu_e2e_ms": 1e3 * gpu_s, "gpu_device_ms": rep.device_ms,
+                     "speedup_e2e": cpu_s / gpu_s, "iterations": rep.iterations, "rel_l2_vs_reference": d,
+                     "cpu_status": st}
+    n = 256
+    u, v, p0 = synthetic.projection_fields(n, seed=17)
+    h = 1.0 / (n - 1)
+    t0 = time.perf_counter()
+    st, ur, vr, _, pr, rrep = oracle.ref_project(u, v, None, p0, n, n, 1, h, h, 1.0, 0.01, 20000, 1e-10)
+    cpu_s = time.perf_counter() - t0
+    solver.project_velocity(u, v, None, p0, n, n, 1, h, h, 1.0, 0.01, 20000, 1e-10)
+    ts = []
+    for _ in range(5):
+        torch_sync()
+        t0 = time.perf_counter()
+        ug, vg, _, pg, rep = solver.project_velocity(u, v, None, p0, n, n, 1, h, h, 1.0, 0.01, 20000, 1e-10)
+        ts.append(time.perf_counter() - t0)
+    gpu_s = statistics.median(ts)
+    out["projection_256"] = {"cpu_ms": 1e3 * cpu_s, "gpu_e2e_ms": 1e3 * gpu_s, "gpu_device_ms": rep.device_ms,
+                             "speedup_e2e": cpu_s / gpu_s, "poisson_iterations": rep.poisson_iterations,
+                             "cpu_poisson_iterations": int(rrep[0]),
+                             "rel_l2_vs_reference": float(np.linalg.norm(pg - pr) / np.linalg.norm(pr))}
+    return out
+
+
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
 
 
 TUNE_CACHE = os.path.join(ROOT, "pde_solver_b200", "batch_tune_cache.txt")
@@ -365,10 +445,10 @@ def bench_convdiff(lib, abi, device, n=513, seed=99, reps=2):
     (eps 1e-2, b a seeded unit vector, F ~ U[-1,1], Dirichlet 0, centred
     convection), MG-preconditioned BiCGStab to 1e-10 relative residual in
     FP32 inside FP64 iterative refinement, beside the same solve in plain
-    FP64; F resident in HBM. The mixed result's error is measured against the
-    FP64 GPU solution (whose parity with the CPU solver is tested at smaller
-    sizes). The coefficients are constants, so there is no coefficient array
-    for BF16 storage."""
+    FP64; F resident in HBM. At 513^3 the mixed result's error is measured
+    against the FP64 GPU solution; `vs_fp64_oracle` measures both GPU results
+    against the FP64 oracle on the same workload at 129^3. The coefficients
+    are constants, so there is no coefficient array for BF16 storage."""
     import copy
 
     import torch
@@ -407,6 +487,77 @@ def bench_convdiff(lib, abi, device, n=513, seed=99, reps=2):
                        f"FP32-in-FP64 refinement vs FP64, F resident in HBM, median of {reps} solves")
     del sols, d, x, f_dev
     torch.cuda.empty_cache()
+    try:
+        out["vs_fp64_oracle"] = convdiff_oracle_check(abi)
+    except Exception as exc:
+        out["vs_fp64_oracle"] = {"error": str(exc)}
+    return out
+
+
+def convdiff_oracle_check(abi, n=129, seed=99):
+    """Error of the GPU results of the convection-diffusion workload against
+    the FP64 oracle at a size the host solves in seconds: the oracle port's
+    unpreconditioned FP64 BiCGStab (oracle/restate.c, all host cores) to 1e-13
+    relative residual on the same 129^3 system."""
+    from oracle import oracle
+    from pde_solver_b200 import solver, synthetic
+    from pde_solver_b200.problem import default_options
+
+    p = synthetic.convection_diffusion_3d(n, seed)
+    oracle.build(ref=False)
+    oracle.restate().rs_set_threads(os.cpu_count() or 1)
+    bnorm = float(np.linalg.norm(p.f.reshape(n, n, n)[1:-1, 1:-1, 1:-1]))
+    t0 = time.perf_counter()
+    st, ref, rrep = oracle.rs_solve(p, default_options(method=abi.BICGSTAB, tol=1e-13 * bnorm, max_iter=20000))
+    cpu_s = time.perf_counter() - t0
+    if st != abi.OK:
+        raise RuntimeError(f"oracle BiCGStab failed: {st}")
+    res = {"grid": f"{n}^3", "oracle": "oracle/restate.c BiCGStab FP64 to 1e-13 rel.", "oracle_iterations":
+           rrep.iterations, "oracle_s": cpu_s}
+    for name, prec, bf16 in (("fp64", abi.FP64, 0), ("mixed", abi.MIXED, 0), ("mixed_bf16", abi.MIXED, 1)):
+        got, rep = solver.solve(p, default_options(method=abi.MG_BICGSTAB, tol=1e-10, tol_mode=abi.TOL_RELATIVE,
+                                                   max_iter=200, precision=prec, bf16_coefficients=bf16))
+        res[name] = {"rel_l2_vs_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                     "rel_residual": rep.rel_residual}
+    return res
+
+
+def summarize(line):
+    """Compact headline figures of every form measured in this run."""
+    f = line.get("forms", {})
+    out = {"fp64_solve_p50_ms": line["latency_ms"]["p50"], "fp64_solve_p99_ms": line["latency_ms"]["p99"]}
+
+    def pick(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return round(d, 6) if isinstance(d, float) else d
+
+    out["batched_solves_per_s"] = pick(f, "batched", "solves_per_s")
+    out["batched_vs_plain_fp64"] = pick(f, "batched", "speedup_vs_plain_fp64")
+    out["batched_e2e_solves_per_s"] = pick(f, "batched", "e2e_solves_per_s")
+    for mode in ("device_resident", "host_inputs"):
+        for prec in ("mixed", "mixed_adaptive", "fp64"):
+            out[f"serving_{mode}_{prec}_solves_per_s"] = pick(f, "serving", mode, prec, "solves_per_s")
+            out[f"serving_{mode}_{prec}_p99_ms"] = pick(f, "serving", mode, prec, "p99_ms")
+    pts = pick(f, "serving_stream", "points") or []
+    for pt in pts:
+        r = int(pt["rate_hz"])
+        for prec in ("mixed", "mixed_adaptive", "fp64"):
+            out[f"stream_{r}hz_{prec}_poisson_p50_ms"] = pick(pt, prec, "poisson_p50_ms")
+            out[f"stream_{r}hz_{prec}_p99_ms"] = pick(pt, prec, "p99_ms")
+    out["convdiff513_fp64_ms"] = pick(f, "convdiff", "fp64", "ms")
+    out["convdiff513_mixed_ms"] = pick(f, "convdiff", "mixed", "ms")
+    out["convdiff513_mixed_rel_l2_vs_gpu_fp64"] = pick(f, "convdiff", "mixed", "rel_l2_vs_fp64")
+    out["convdiff129_mixed_rel_l2_vs_fp64_oracle"] = pick(f, "convdiff", "vs_fp64_oracle", "mixed", "rel_l2_vs_oracle")
+    out["convdiff129_fp64_rel_l2_vs_fp64_oracle"] = pick(f, "convdiff", "vs_fp64_oracle", "fp64", "rel_l2_vs_oracle")
+    for k in ("config1_cg_129", "config1_jacobi_129", "projection_256"):
+        out[f"{k}_gpu_e2e_ms"] = pick(f, "reference_code", k, "gpu_e2e_ms")
+        out[f"{k}_reference_cpu_ms"] = pick(f, "reference_code", k, "cpu_ms")
+        out[f"{k}_rel_l2_vs_reference"] = pick(f, "reference_code", k, "rel_l2_vs_reference")
+    out["vtk_legacy_ms"] = pick(f, "output", "vtk_legacy", "ms")
+    out["cpu_baseline_solves_per_s"] = pick(line, "cpu_baseline", "value")
     return out
 
 
@@ -489,51 +640,32 @@ def bench_serving_stream(abi, rates=(50.0, 100.0, 200.0), count=64, seed=11):
 
 
 def run_reference(args):
+    """The CPU implementation of the headline workload on the host cores: each
+    step is one whole converged 257^3 solve by the oracle port of the same
+    MG-PCG (oracle/restate.c; the reference's CPU path has no 3D divergence-form
+    solver), W warm-up solves then exactly K timed ones."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import oracle
-    from pde_solver_b200 import abi, synthetic
-    from pde_solver_b200.problem import default_options
+    from pde_solver_b200 import synthetic
 
-    cores = os.cpu_count() or 1
-    oracle.build(ref=False)
-    oracle.restate().rs_set_threads(cores)
     prob = synthetic.varcoef_poisson_3d(args.n, seed=SEED)
-    full = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=400)
-    # warm-up: one converged solve fixes the iteration count of this input
-    t0 = time.perf_counter()
-    st, _, rep = oracle.rs_solve(prob, full)
-    t_full = time.perf_counter() - t0
-    iters = rep.iterations
-    one = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=1)
-    three = default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=3)
-    for _ in range(max(args.warmup - 1, 0)):
-        oracle.rs_solve(prob, one)
-    t3 = []
-    t0 = time.perf_counter()
-    oracle.rs_solve(prob, three)
-    t3.append(time.perf_counter() - t0)
-    samples = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        oracle.rs_solve(prob, one)
-        samples.append(time.perf_counter() - t0)
-    t1 = statistics.median(samples)
-    t_iter = max((t3[0] - t1) / 2.0, 1e-9)
-    t_solve = max(t1 - t_iter, 0.0) + iters * t_iter
-    value = 1.0 / t_solve
+    if args.warmup > 0:
+        cpu_solve_times(prob, args.warmup)
+    times, iters, cores = cpu_solve_times(prob, args.steps)
+    total = sum(times)
+    value = args.steps / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_solve, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": config(args.n, "cpu"),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": config(args.n, "cpu"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": (f"oracle/restate.c MG-PCG (the reference's CPU path has no 3D "
-                                    f"divergence-form MG-PCG), {cores} OpenMP threads; one converged solve "
-                                    f"({iters} iterations, {t_full:.1f}s) in warm-up, each step = setup + 1 "
-                                    f"iteration, solve = setup + {iters} iterations")},
+                                    f"divergence-form MG-PCG), {cores} OpenMP threads; each step one whole "
+                                    f"converged solve ({iters} iterations)")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": 1e3 * _pct(times, 50), "p99": 1e3 * _pct(times, 99)},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -614,6 +746,8 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
+    latency = {"p50": _pct(step_dev, 50), "p99": _pct(step_dev, 99), "max": max(step_dev),
+               "over": "device time of each timed solve"}
     ms = replicas.max_over_ranks(ms, dist, device)
     value = replicas.aggregate_rate(world, args.steps, ms)
 
@@ -682,7 +816,7 @@ def main():
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded, generated on the host)",
         "config": config(n, "inputs larger than L2 (k, f, x, r, p, q: 136 MB each)"),
-        "iterations": iters, "rel_residual": rel, "dof_iterations_per_s": N * iters * value,
+        "iterations": iters, "rel_residual": rel, "dof_iterations_per_s": N * iters * value, "latency_ms": latency,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8,
                 "matches_device_result": bool(ok_host)},
         "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
@@ -695,7 +829,8 @@ def main():
         for key, run in (("batched", lambda: bench_batched(lib, abi)), ("serving", lambda: bench_serving(abi)),
                          ("serving_stream", lambda: bench_serving_stream(abi)),
                          ("output", lambda: bench_output(out_dev, n)),
-                         ("convdiff", lambda: bench_convdiff(lib, abi, device))):
+                         ("convdiff", lambda: bench_convdiff(lib, abi, device)),
+                         ("reference_code", lambda: reference_code_paths(lib, abi, device))):
             try:
                 forms[key] = run()
             except Exception as exc:  # the forms never block the headline line
@@ -703,10 +838,13 @@ def main():
         line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_sample(prob, iters)
+            line["cpu_baseline"] = cpu_sample(prob)
         except Exception as exc:  # the baseline never blocks the GPU line
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {exc}"}
+    if "forms" in line:
+        # the forms' headline figures, last in the line so a kept tail holds them
+        line["summary"] = summarize(line)
     lib.pdeb200_set_stream(local, None)
     if rank == 0:
         print(json.dumps(line), flush=True)

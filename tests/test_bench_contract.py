@@ -51,3 +51,30 @@ def test_nearest_rank_percentile():
     xs = list(range(1, 101))
     assert bench._pct(xs, 99) == 99 and bench._pct(xs, 100) == 100 and bench._pct(xs, 1) == 1
     assert bench._pct(list(range(1, 65)), 50) == 32
+
+
+def test_reference_arm_steps_are_whole_solves():
+    # each step is one whole converged solve: K steps take K x ms_per_step,
+    # which fits inside the process's own wall time
+    import time
+
+    t0 = time.perf_counter()
+    p = run_bench("--impl", "reference", "--steps", "3", "--warmup", "1", "--n", "33")
+    wall = time.perf_counter() - t0
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["steps"] * line["ms_per_step"] / 1e3 <= wall
+    assert "whole converged solve" in line["cpu_baseline"]["sample"]
+    lat = line["latency_ms"]
+    assert 0 < lat["p50"] <= lat["p99"]
+
+
+def test_summary_picks_form_figures():
+    import bench
+
+    line = {"latency_ms": {"p50": 23.0, "p99": 24.0}, "cpu_baseline": {"value": 0.1},
+            "forms": {"batched": {"solves_per_s": 7000.0, "speedup_vs_plain_fp64": 19.0},
+                      "serving_stream": {"points": [{"rate_hz": 50.0, "fp64": {"poisson_p50_ms": 5.0, "p99_ms": 9.0}}]}}}
+    s = bench.summarize(line)
+    assert s["fp64_solve_p50_ms"] == 23.0 and s["batched_vs_plain_fp64"] == 19.0
+    assert s["stream_50hz_fp64_poisson_p50_ms"] == 5.0 and s["serving_host_inputs_mixed_solves_per_s"] is None
