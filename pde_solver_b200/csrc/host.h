@@ -230,6 +230,8 @@ dim3 stencil_grid_auto(const GridDev& g, long long target_blocks = 0);
 inline dim3 rbgs_grid(const GridDev& g) { return stencil_grid_auto(g, 148 * 9); }
 // launch shape of the fused red-black sweep (64 x 8 column tiles)
 dim3 fused_grid(const GridDev& g);
+// launch shape of the marching single-pass sweep (64 x 8 interior column tiles, z chunks)
+dim3 march_grid(const GridDev& g);
 // launch shape of the staged single-pass sweep (32 x 8 column tiles, z chunks
 // for about four resident blocks per SM over two waves)
 dim3 sweep_grid(const GridDev& g);

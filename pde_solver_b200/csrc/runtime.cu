@@ -1,11 +1,13 @@
 // Runtime of libpdeb200: device contexts, problem upload, face closures and
 // the extern "C" entry points declared in include/pdeb200.h.
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <limits>
 
 #include "host.h"
+#include "march.cuh"
 
 namespace pdeb {
 
@@ -145,6 +147,25 @@ dim3 fused_grid(const GridDev& g) {
   if (chunks > max_chunks) chunks = max_chunks;
   if (chunks < 1) chunks = 1;
   return dim3(xy.x, xy.y, cap_chunks(xyb, (int)chunks));
+}
+
+dim3 march_grid(const GridDev& g) {
+  // about `waves` waves of the two resident blocks per SM its shared memory
+  // allows, at least 16 planes per chunk (each chunk re-reads 3 planes)
+  static const int waves = [] {
+    const char* e = std::getenv("PDEB200_MARCH_WAVES");
+    const int w = e ? std::atoi(e) : 3;
+    return w > 0 ? w : 3;
+  }();
+  const long long target = 148LL * 2 * waves;
+  const int kint = g.nz - 2;
+  const dim3 xy((g.nx - 2 + kMTx - 1) / kMTx, (g.ny - 2 + kMTy - 1) / kMTy, 1);
+  const long long xyb = (long long)xy.x * xy.y;
+  long long chunks = (target + xyb - 1) / xyb;
+  const long long max_chunks = (kint + 15) / 16;
+  if (chunks > max_chunks) chunks = max_chunks;
+  if (chunks < 1) chunks = 1;
+  return dim3(xy.x, xy.y, (unsigned)chunks);
 }
 
 dim3 stencil_grid_full(const GridDev& g, int zchunk) {

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "host.h"
+#include "march.cuh"
 #include "sweep.cuh"
 
 namespace pdeb {
@@ -474,6 +475,7 @@ struct Hierarchy {
     T* r;
     T* out;  // buffer holding this level's result after a V-cycle
     bool single_pass = false;  // sweeps by k_rbgs_sweep (x_in -> x_out) instead of colour passes
+    bool march = false;        // sweeps by k_rbgs_march (x_in -> x_out) instead of colour passes
   };
   // With PDEB200_STAGED_SWEEP set, levels with at least this many nodes use
   // the staged single-pass sweep (FP64 constant or divergence-form
@@ -481,6 +483,10 @@ struct Hierarchy {
   // B200 it is issue- and barrier-bound and about 10% slower at 257^3, so the
   // colour passes stay the default.
   static constexpr long long kSweepMinNodes = 1LL << 18;
+  // Levels of at least kMarchMinNodes nodes (3D, FP64, constant or
+  // divergence-form coefficients) smooth with the single-pass marching sweep
+  // (k_rbgs_march) unless PDEB200_NO_MARCH is set.
+  static constexpr long long kMarchMinNodes = 1LL << 18;
   static constexpr bool kSweepCoef =
       std::is_same<T, double>::value &&
       (std::is_same<Coef, CoefConst>::value || std::is_same<Coef, CoefDivk<double>>::value);
@@ -569,11 +575,14 @@ struct Hierarchy {
     // result buffer of each level after a V-cycle (fixed, so launches can be captured):
     // the first sweep from zero writes xa, every later sweep flips the buffer
     const bool sweep_env = std::getenv("PDEB200_STAGED_SWEEP") != nullptr;
+    const bool march_env = std::getenv("PDEB200_NO_MARCH") == nullptr;
     for (size_t l = 0; l < levels.size(); ++l) {
       Level& L = levels[l];
       L.single_pass = kSweepCoef && sweep_env && !fused && l + 1 < levels.size() && L.g.dim == 3 &&
                       L.g.n >= kSweepMinNodes;
-      if (!fused && !L.single_pass) {
+      L.march = kSweepCoef && march_env && !fused && !L.single_pass && l + 1 < levels.size() && L.g.dim == 3 &&
+                L.g.n >= kMarchMinNodes;
+      if (!fused && !L.single_pass && !L.march) {
         L.out = L.xa;
         continue;
       }
@@ -592,11 +601,40 @@ struct Hierarchy {
   // buffer and write the other.
   bool fused = false;
   T* sweeps_from(Context* ctx, Level& L, const T* b, T* cur, int sweeps, int first, bool from_zero,
-                 const Ctl* ctl, int lvl) {
+                 const Ctl* ctl, int lvl, const RedSlot* dot_last = nullptr) {
     const dim3 grid = rbgs_grid(L.g), block = stencil_block();
     const dim3 zgrid = stencil_grid_auto(L.g);  // the pass from zero (fewer registers) keeps the default
     const double dofs = interior_dofs(L.g);
     if constexpr (kSweepCoef) {
+      if (L.march) {
+        constexpr size_t smem = march_smem_bytes<Coef>();
+        static bool attr_set[64] = {false};
+        const int dv = ctx->dev >= 0 && ctx->dev < 64 ? ctx->dev : 0;
+        if (!attr_set[dv]) {
+          PDEB_CUDA(cudaFuncSetAttribute(k_rbgs_march<Coef, false, NoPost>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          PDEB_CUDA(cudaFuncSetAttribute(k_rbgs_march<Coef, true, PostBeta>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          attr_set[dv] = true;
+        }
+        const dim3 mgrid = march_grid(L.g);
+        for (int s = 0; s < sweeps; ++s) {
+          const bool zero = from_zero && s == 0;
+          T* in = zero ? L.xb : cur;
+          T* out = zero ? L.xa : (cur == L.xa ? L.xb : L.xa);
+          // x read and written once, b and k read once: 32 B per DOF (24 from zero)
+          ProfScope ps(ctx, zero ? "march_sweep_zero" : "march_sweep", lvl, dofs * (zero ? 3.0 : 4.0) * sizeof(T));
+          if (dot_last && s + 1 == sweeps)
+            k_rbgs_march<Coef, true, PostBeta><<<mgrid, kMThreads, smem, ctx->stream>>>(
+                L.g, L.cf, b, in, out, first, zero ? 1 : 0, ctl, *dot_last, PostBeta{const_cast<Ctl*>(ctl)});
+          else
+            k_rbgs_march<Coef><<<mgrid, kMThreads, smem, ctx->stream>>>(L.g, L.cf, b, in, out, first, zero ? 1 : 0,
+                                                                         ctl);
+          ctx->count();
+          cur = out;
+        }
+        return cur;
+      }
       if (L.single_pass) {
         // per instantiation and device, before its first launch there
         static bool attr_set[64] = {false};
@@ -731,7 +769,11 @@ struct Hierarchy {
         k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
     }
     ctx->count();
-    if (l == 0 && dot_slot && post > 0 && !fused && !L.single_pass) {
+    if (l == 0 && dot_slot && post > 0 && L.march) {
+      // the last sweep also sums r.z (b is r on level 0) and forms beta
+      cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l, dot_slot);
+      dot_done = true;
+    } else if (l == 0 && dot_slot && post > 0 && !fused && !L.single_pass) {
       // the last sweep's two passes also sum r.z (b is r on level 0)
       cur = sweeps_from(ctx, L, b, cur, post - 1, 1, false, ctl, l);
       const dim3 grid = rbgs_grid(L.g), block = stencil_block();

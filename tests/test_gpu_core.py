@@ -240,3 +240,32 @@ def test_staged_sweep_matches_colour_passes(monkeypatch, which):
     b, rb = solver.solve(p, opt)
     assert abs(ra.iterations - rb.iterations) <= 1
     assert rel_l2(a, b) <= 1e-10
+
+
+@pytest.mark.parametrize("which", ["divk", "const", "uneven"])
+def test_marching_sweep_matches_colour_passes(monkeypatch, which):
+    # levels of 2^18+ nodes smooth with the single-pass marching sweep
+    # (k_rbgs_march); it does the arithmetic of two colour passes, so the
+    # solve agrees with the colour-pass form to rounding at the same
+    # iteration count
+    if which == "divk":
+        p = synthetic.varcoef_poisson_3d(65, seed=21)
+    elif which == "const":
+        p = GridProblem(65, 70, 66, a=-1.0, b=-1.0, az=-1.0, c=0.2)
+        p.f = np.random.Generator(np.random.PCG64(2)).standard_normal(p.n)
+        p.faces = [FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(1.0),
+                   FaceBC.neumann(0.1), FaceBC.dirichlet(0.0)]
+    else:
+        rng = np.random.Generator(np.random.PCG64(8))
+        p = GridProblem(131, 37, 70, coef_kind=abi.COEF_DIVK)
+        p.k = np.exp(0.5 * rng.standard_normal(p.n))
+        p.f = rng.standard_normal(p.n)
+        p.faces = [FaceBC.robin(2.0, 0.02, 0.0), FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.dirichlet(0.5),
+                   FaceBC.dirichlet(0.0), FaceBC.neumann(0.2)]
+    opt = default_options(method=abi.MG_PCG, tol=1e-11, tol_mode=abi.TOL_RELATIVE, max_iter=200)
+    a, ra = solver.solve(p, opt)
+    monkeypatch.setenv("PDEB200_NO_MARCH", "1")
+    b, rb = solver.solve(p, opt)
+    assert ra.status == abi.OK and rb.status == abi.OK
+    assert ra.iterations == rb.iterations
+    assert rel_l2(a, b) <= 1e-12
