@@ -483,9 +483,13 @@ struct Hierarchy {
   // B200 it is issue- and barrier-bound and about 10% slower at 257^3, so the
   // colour passes stay the default.
   static constexpr long long kSweepMinNodes = 1LL << 18;
-  // Levels of at least kMarchMinNodes nodes (3D, FP64, constant or
-  // divergence-form coefficients) smooth with the single-pass marching sweep
-  // (k_rbgs_march) unless PDEB200_NO_MARCH is set.
+  // With PDEB200_MARCH set, levels of at least kMarchMinNodes nodes (3D,
+  // FP64, constant or divergence-form coefficients) smooth with the
+  // single-pass marching sweep (k_rbgs_march). It moves 552 MB per sweep at
+  // 257^3 against 2 x 512 MB for two colour passes, but it is latency- and
+  // barrier-bound (about 21 warps per SM, one barrier per plane): 255 against
+  // 226 us per sweep on a box where a colour pass takes 113 us, so the colour
+  // passes stay the default.
   static constexpr long long kMarchMinNodes = 1LL << 18;
   static constexpr bool kSweepCoef =
       std::is_same<T, double>::value &&
@@ -575,7 +579,7 @@ struct Hierarchy {
     // result buffer of each level after a V-cycle (fixed, so launches can be captured):
     // the first sweep from zero writes xa, every later sweep flips the buffer
     const bool sweep_env = std::getenv("PDEB200_STAGED_SWEEP") != nullptr;
-    const bool march_env = std::getenv("PDEB200_NO_MARCH") == nullptr;
+    const bool march_env = std::getenv("PDEB200_MARCH") != nullptr;
     for (size_t l = 0; l < levels.size(); ++l) {
       Level& L = levels[l];
       L.single_pass = kSweepCoef && sweep_env && !fused && l + 1 < levels.size() && L.g.dim == 3 &&

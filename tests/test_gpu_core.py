@@ -244,10 +244,10 @@ def test_staged_sweep_matches_colour_passes(monkeypatch, which):
 
 @pytest.mark.parametrize("which", ["divk", "const", "uneven"])
 def test_marching_sweep_matches_colour_passes(monkeypatch, which):
-    # levels of 2^18+ nodes smooth with the single-pass marching sweep
-    # (k_rbgs_march); it does the arithmetic of two colour passes, so the
-    # solve agrees with the colour-pass form to rounding at the same
-    # iteration count
+    # with PDEB200_MARCH, levels of 2^18+ nodes smooth with the single-pass
+    # marching sweep (k_rbgs_march); it does the arithmetic of two colour
+    # passes, so the solve agrees with the colour-pass form to rounding at the
+    # same iteration count
     if which == "divk":
         p = synthetic.varcoef_poisson_3d(65, seed=21)
     elif which == "const":
@@ -263,9 +263,9 @@ def test_marching_sweep_matches_colour_passes(monkeypatch, which):
         p.faces = [FaceBC.robin(2.0, 0.02, 0.0), FaceBC.dirichlet(0.0), FaceBC.neumann(0.0), FaceBC.dirichlet(0.5),
                    FaceBC.dirichlet(0.0), FaceBC.neumann(0.2)]
     opt = default_options(method=abi.MG_PCG, tol=1e-11, tol_mode=abi.TOL_RELATIVE, max_iter=200)
-    a, ra = solver.solve(p, opt)
-    monkeypatch.setenv("PDEB200_NO_MARCH", "1")
     b, rb = solver.solve(p, opt)
+    monkeypatch.setenv("PDEB200_MARCH", "1")
+    a, ra = solver.solve(p, opt)
     assert ra.status == abi.OK and rb.status == abi.OK
     assert ra.iterations == rb.iterations
     assert rel_l2(a, b) <= 1e-12
