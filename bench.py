@@ -532,7 +532,7 @@ def summarize(line):
             if not isinstance(d, dict) or k not in d:
                 return None
             d = d[k]
-        return round(d, 6) if isinstance(d, float) else d
+        return float(f"{d:.6g}") if isinstance(d, float) else d
 
     out["batched_solves_per_s"] = pick(f, "batched", "solves_per_s")
     out["batched_vs_plain_fp64"] = pick(f, "batched", "speedup_vs_plain_fp64")

@@ -430,9 +430,19 @@ pdeb200_status project_dev(Context* ctx, int nx, int ny, int nz, double dx, doub
     k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, pc, r, C, 0);
     ctx->count(2);
   };
+  // the iteration is captured once as a CUDA graph and replayed (projection
+  // sizes are launch-bound: 256^2 takes about 24 us per iteration as direct launches)
+  IterGraph graph;
+  const bool graphed = graph.capture(ctx, iterate);
+  auto step = [&](int it) {
+    if (graphed)
+      graph.launch(ctx);
+    else
+      iterate(it);
+  };
   pdeb200_options o{};
   o.check_interval = 32;
-  pdeb200_status st = drive(ctx, &o, po->max_iter + 1, iterate, false);
+  pdeb200_status st = drive(ctx, &o, po->max_iter + 1, step, false);
   const Ctl c = ctl_poll(ctx);
   const bool zero_start = c.aux[4] != 0.0;
   const bool breakdown = c.aux[7] != 0.0;

@@ -39,7 +39,23 @@ pdeb200_status jacobi(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
     fill_boundary(ctx, g, dst, ctx->d_ctl);
     ctx->count();
   };
-  pdeb200_status st = drive(ctx, o, max_iter, iterate, true);
+  // kJacobiGroup sweeps (an even number, so each group starts from buf[0])
+  // captured once as a CUDA graph and replayed: small grids are launch-bound
+  // (129^2: about 11 us per sweep as two direct launches). Sweeps after the
+  // stopping test fired return at once, so a group may end past it.
+  constexpr int kJacobiGroup = 8;
+  auto group = [&](int) {
+    for (int t = 0; t < kJacobiGroup; ++t) iterate(t);
+  };
+  IterGraph graph;
+  const bool graphed = graph.capture(ctx, group);
+  auto step = [&](int q) {
+    if (graphed)
+      graph.launch(ctx);
+    else
+      group(q);
+  };
+  pdeb200_status st = drive(ctx, o, (max_iter + kJacobiGroup - 1) / kJacobiGroup, step, true);
   const Ctl c = ctl_poll(ctx);
   int dg = 0;
   PDEB_CUDA(cudaMemcpy(&dg, degen.as<int>(), sizeof(int), cudaMemcpyDeviceToHost));

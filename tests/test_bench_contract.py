@@ -74,7 +74,9 @@ def test_summary_picks_form_figures():
 
     line = {"latency_ms": {"p50": 23.0, "p99": 24.0}, "cpu_baseline": {"value": 0.1},
             "forms": {"batched": {"solves_per_s": 7000.0, "speedup_vs_plain_fp64": 19.0},
+                      "convdiff": {"mixed": {"rel_l2_vs_fp64": 3.41e-09}},
                       "serving_stream": {"points": [{"rate_hz": 50.0, "fp64": {"poisson_p50_ms": 5.0, "p99_ms": 9.0}}]}}}
     s = bench.summarize(line)
     assert s["fp64_solve_p50_ms"] == 23.0 and s["batched_vs_plain_fp64"] == 19.0
     assert s["stream_50hz_fp64_poisson_p50_ms"] == 5.0 and s["serving_host_inputs_mixed_solves_per_s"] is None
+    assert s["convdiff513_mixed_rel_l2_vs_gpu_fp64"] == 3.41e-09  # small values keep their digits
