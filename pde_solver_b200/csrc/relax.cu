@@ -274,120 +274,6 @@ pdeb200_status gauss_seidel(Context* ctx, DevProblem& P, const Coef& cf, const p
   return st;
 }
 
-// Whole Jacobi solve in one resident block for small grids (the reference's
-// sequence: sweep grid -> next with max|du|, closures on next, swap; stop on
-// max|du| < tol, a degenerate centre or max_iter). Per sweep the nodes are
-// updated with k_jacobi's arithmetic; two launches per sweep would cost more
-// than the sweep itself at these sizes. Bounded by a device-time budget like
-// k_gs_lex_block.
-template <class Coef>
-__global__ void __launch_bounds__(1024) k_jacobi_block(GridDev g, Coef cf, const double* __restrict__ f, double fc,
-                                                       NonlinDev nl, double* u0, double* u1, double tol,
-                                                       int max_iter, unsigned long long budget_ns, Ctl* ctl) {
-  __shared__ double red[32];
-  __shared__ int s_stop;
-  __shared__ int s_degen;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    s_stop = 0;
-    s_degen = 0;
-  }
-  __syncthreads();
-  const unsigned long long t0 = globaltimer_ns();
-  const int ix = g.nx - 2, iy = g.ny - 2, iz = g.dim == 3 ? g.nz - 2 : 1;
-  const long long interior = (long long)ix * iy * iz;
-  double* cur = u0;
-  double* nxt = u1;
-  int it = 0;
-  double delta_out = 0.0;
-  for (it = 0; it < max_iter; ++it) {
-    double delta = 0.0;
-    int degen = 0;
-    for (long long t = tid; t < interior; t += blockDim.x) {
-      const int i = 1 + int(t % ix);
-      const int j = 1 + int((t / ix) % iy);
-      const int k = g.dim == 3 ? 1 + int(t / ((long long)ix * iy)) : 0;
-      const long long id = ((long long)k * g.ny + j) * g.nx + i;
-      const Stencil<double> s = cf.template at<double>(g, id);
-      if (fabs(s.c) < 1e-12) {
-        degen = 1;
-        continue;
-      }
-      const double zp = g.dim == 3 ? cur[id + g.sxy] : 0.0;
-      const double zm = g.dim == 3 ? cur[id - g.sxy] : 0.0;
-      const double lap = nb_sum<double>(s, cur[id + 1], cur[id - 1], cur[id + g.nx], cur[id - g.nx], zp, zm, g.dim);
-      const double old_u = cur[id];
-      const double rhs = -f_plus_nl(f ? f[id] : fc, nl, old_u) - lap;
-      const double upd = __ddiv_rn(rhs, s.c);
-      nxt[id] = upd;
-      delta = fmax(delta, fabs(upd - old_u));
-    }
-    if (degen) s_degen = 1;
-    __syncthreads();
-    block_fill_boundary(g, nxt, true);
-    // block max of delta
-    for (int off = 16; off > 0; off >>= 1) delta = fmax(delta, __shfl_down_sync(0xffffffffu, delta, off));
-    if ((tid & 31) == 0) red[tid >> 5] = delta;
-    __syncthreads();
-    if (tid < 32) {
-      double v = tid < (int)(blockDim.x + 31) / 32 ? red[tid] : 0.0;
-      for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-      if (tid == 0) red[0] = v;
-    }
-    __syncthreads();
-    const double md = red[0];
-    delta_out = md;
-    if (tid == 0) {
-      if (s_degen) s_stop = 2;
-      else if (md < tol) s_stop = 1;
-      else if (globaltimer_ns() - t0 > budget_ns) s_stop = 3;
-    }
-    __syncthreads();
-    double* tmp = cur;
-    cur = nxt;
-    nxt = tmp;
-    if (s_stop) break;
-  }
-  if (tid == 0) {
-    const int stop = s_stop;
-    int status = PDEB200_ERR_NOT_CONVERGED;
-    if (stop == 1) status = PDEB200_OK;
-    else if (stop == 2) status = PDEB200_ERR_DEGENERATE;
-    else if (stop == 3) status = PDEB200_ERR_TIMEOUT;
-    ctl->iter = stop ? it + 1 : it;
-    ctl->delta = delta_out;
-    ctl->status = status;
-    ctl->done = 1;
-  }
-}
-
-// Jacobi of a grid with at most kJacobiBlockMax interior nodes in one block;
-// u0 holds the initial closures, u1 is scratch. The result is in u0 when the
-// iteration count is even, else in u1 (the caller copies it back).
-template <class Coef>
-pdeb200_status jacobi_block(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o, double* u0,
-                            double* u1, int max_iter, pdeb200_report* rep) {
-  const unsigned long long budget = 60ULL * 1000000000ULL;  // device-time guard: 60 s
-  k_jacobi_block<Coef><<<1, 1024, 0, ctx->stream>>>(P.g, cf, P.f, P.f_const, P.nl, u0, u1, o->tol, max_iter, budget,
-                                                    ctx->d_ctl);
-  ctx->count();
-  const Ctl& c = ctl_poll(ctx);
-  if (rep) {
-    rep->iterations = c.iter;
-    rep->last_delta = c.delta;
-    rep->converged = c.status == PDEB200_OK;
-  }
-  return (pdeb200_status)c.status;
-}
-
-template pdeb200_status jacobi_block<CoefConst>(Context*, DevProblem&, const CoefConst&, const pdeb200_options*,
-                                                double*, double*, int, pdeb200_report*);
-template pdeb200_status jacobi_block<CoefDivk<double>>(Context*, DevProblem&, const CoefDivk<double>&,
-                                                       const pdeb200_options*, double*, double*, int,
-                                                       pdeb200_report*);
-template pdeb200_status jacobi_block<CoefNodal>(Context*, DevProblem&, const CoefNodal&, const pdeb200_options*,
-                                                double*, double*, int, pdeb200_report*);
-
 template pdeb200_status gauss_seidel<CoefConst>(Context*, DevProblem&, const CoefConst&, const pdeb200_options*,
                                                 double*, pdeb200_report*);
 template pdeb200_status gauss_seidel<CoefDivk<double>>(Context*, DevProblem&, const CoefDivk<double>&,

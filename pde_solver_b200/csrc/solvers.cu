@@ -6,7 +6,6 @@
 // reduction and convergence is decided on the device (Ctl), so the host only
 // enqueues and polls.
 #include <cmath>
-#include <cstdlib>
 #include <cstring>
 
 #include "host.h"
@@ -31,16 +30,6 @@ pdeb200_status jacobi(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
   PDEB_CUDA(cudaMemsetAsync(buf[1], 0, sizeof(double) * g.n, ctx->stream));
   ctl_init(ctx, max_iter, o->tol, 0.0);
   fill_boundary(ctx, g, buf[0], ctx->d_ctl);
-  const long long interior = (long long)(g.nx - 2) * (g.ny - 2) * (g.dim == 3 ? g.nz - 2 : 1);
-  if (interior <= kJacobiBlockMax && std::getenv("PDEB200_NO_JACOBI_BLOCK") == nullptr) {
-    // small grids: the whole solve in one resident block
-    const pdeb200_status st = jacobi_block(ctx, P, cf, o, buf[0], buf[1], max_iter, rep);
-    if (st == PDEB200_ERR_DEGENERATE) return st;
-    // the result is in buf[iter & 1]
-    if (ctl_poll(ctx).iter & 1)
-      PDEB_CUDA(cudaMemcpyAsync(d_out, buf[1], sizeof(double) * g.n, cudaMemcpyDeviceToDevice, ctx->stream));
-    return st;
-  }
   const dim3 grid = stencil_grid(g), block = stencil_block();
   auto iterate = [&](int t) {
     double* src = buf[t & 1];

@@ -823,11 +823,6 @@ struct Hierarchy {
 template <class Coef>
 pdeb200_status gauss_seidel(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o, double* d_out,
                             pdeb200_report* rep);
-// whole Jacobi solve in one block (grids of at most kJacobiBlockMax interior nodes)
-constexpr long long kJacobiBlockMax = 1LL << 16;
-template <class Coef>
-pdeb200_status jacobi_block(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o, double* u0,
-                            double* u1, int max_iter, pdeb200_report* rep);
 template <class Coef>
 pdeb200_status bicgstab_reference(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200_options* o,
                                   double* d_x, pdeb200_report* rep);

@@ -269,22 +269,3 @@ def test_marching_sweep_matches_colour_passes(monkeypatch, which):
     assert ra.status == abi.OK and rb.status == abi.OK
     assert ra.iterations == rb.iterations
     assert rel_l2(a, b) <= 1e-12
-
-
-@pytest.mark.parametrize("dims,nl", [((41, 37, 1), False), ((17, 15, 13), False), ((33, 29, 1), True)])
-def test_single_block_jacobi_matches_graph_launches(monkeypatch, dims, nl):
-    # grids of at most 2^16 interior nodes run the whole Jacobi solve in one
-    # block; the sweeps do k_jacobi's arithmetic, so fields and counts are identical
-    p = GridProblem(*dims, a=-1.0, b=-1.0, az=-1.0, c=0.3)
-    p.faces = mixed_faces_2d() if dims[2] == 1 else mixed_faces_3d()
-    p.f = np.random.Generator(np.random.PCG64(sum(dims))).standard_normal(p.n)
-    if nl:
-        p.nonlinear = [(abi.NL_POWER, 0.5, 2), (abi.NL_SIN, 1.0, 2)]
-    for tol, max_iter in ((1e-11, 100000), (0.0, 301), (0.0, 300)):
-        opt = default_options(method=abi.JACOBI, max_iter=max_iter, tol=tol)
-        a, ra = solver.solve(p, opt)
-        monkeypatch.setenv("PDEB200_NO_JACOBI_BLOCK", "1")
-        b, rb = solver.solve(p, opt)
-        monkeypatch.delenv("PDEB200_NO_JACOBI_BLOCK")
-        assert ra.status == rb.status and ra.iterations == rb.iterations
-        assert np.array_equal(a, b)
