@@ -43,10 +43,10 @@ __device__ __forceinline__ bool ctl_stopped(const Ctl* c) {
   return c && (*((volatile const int*)&c->done) || *((volatile const int*)&c->stop));
 }
 
-__device__ __forceinline__ void column_range(const GridDev& g, int& k0, int& k1, int zb = 0, int ze = 0) {
-  // interior z range (or the planes [zb, ze) of it when ze > zb) split into gridDim.z chunks
-  const int kb = ze > zb ? zb : (g.dim == 3 ? 1 : 0);
-  const int ke = ze > zb ? ze : (g.dim == 3 ? g.nz - 1 : 1);
+__device__ __forceinline__ void column_range(const GridDev& g, int& k0, int& k1) {
+  // interior z range split into gridDim.z chunks
+  const int kb = g.dim == 3 ? 1 : 0;
+  const int ke = g.dim == 3 ? g.nz - 1 : 1;
   const int len = ke - kb;
   const int chunk = (len + gridDim.z - 1) / gridDim.z;
   k0 = kb + blockIdx.z * chunk;
@@ -194,17 +194,15 @@ __global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, con
 // DOT: the sum over the updated nodes of b * (new x) is reduced over the grid
 // and handed to `post` (the last two passes of a V-cycle's finest level give
 // r.z of preconditioned CG, since b is r there).
-// zb, ze: with ze > zb only the interior planes [zb, ze) are updated (the
-// slab schedule of large levels, Hierarchy::sweeps_from).
 template <class Coef, typename T, typename TB, bool ZERO = false, bool DOT = false, class Post = NoPost>
 __global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x,
                                                    int color, const Ctl* ctl, RedSlot slot = RedSlot{},
-                                                   Post post = Post{}, int zb = 0, int ze = 0) {
+                                                   Post post = Post{}) {
   if (ctl_skip(ctl)) return;
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
   int k0, k1;
-  column_range(g, k0, k1, zb, ze);
+  column_range(g, k0, k1);
   double acc[1] = {0.0};
   // with DOT every thread reaches the block reduction at the end
   if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) {

@@ -109,11 +109,6 @@ struct PostBetaSplit {
     c->rz = rz;
   }
 };
-// slab schedule: the launches between the first and the last add their part
-struct PostRZAdd {
-  Ctl* c;
-  __device__ void operator()(const double* v) const { c->aux[kAuxRzPart] += v[0]; }
-};
 
 // |b|^2 of the relative rule: tol2 = tol^2 |b|^2, immediate exit for b = 0
 struct PostBB {
@@ -481,7 +476,6 @@ struct Hierarchy {
     T* out;  // buffer holding this level's result after a V-cycle
     bool single_pass = false;  // sweeps by k_rbgs_sweep (x_in -> x_out) instead of colour passes
     bool march = false;        // sweeps by k_rbgs_march (x_in -> x_out) instead of colour passes
-    int slab = 0;              // > 0: colour passes in z slabs of this many planes (slab schedule)
   };
   // With PDEB200_STAGED_SWEEP set, levels with at least this many nodes use
   // the staged single-pass sweep (FP64 constant or divergence-form
@@ -592,7 +586,6 @@ struct Hierarchy {
                       L.g.n >= kSweepMinNodes;
       L.march = kSweepCoef && march_env && !fused && !L.single_pass && l + 1 < levels.size() && L.g.dim == 3 &&
                 L.g.n >= kMarchMinNodes;
-      L.slab = (!fused && !L.single_pass && !L.march && l + 1 < levels.size()) ? slab_planes(L.g) : 0;
       if (!fused && !L.single_pass && !L.march) {
         L.out = L.xa;
         continue;
@@ -604,73 +597,6 @@ struct Hierarchy {
         flips = pre > 0 ? pre - 1 + post : post;
       L.out = (flips & 1) ? L.xb : L.xa;
     }
-  }
-
-  // Slab schedule of a sweep on a level whose x, k and b do not fit in L2
-  // together: the interior planes are cut into slabs whose x, k and b do
-  // (about kSlabBytes), and each slab's first-colour pass is followed at once
-  // by the second-colour pass of the planes below its last one, which finds
-  // x, k and b in L2. The second colour of a plane needs the first colour of
-  // the planes above and below it, so the second-colour launches trail the
-  // first-colour ones by one plane; the first colour of a slab reads only
-  // second-colour values not updated yet. Every node gets the update of the
-  // two whole-grid colour passes, in the same arithmetic (k_rbgs with a
-  // z range); only the launch order differs. PDEB200_NO_SLABS turns it off.
-  static constexpr double kSlabBytes = 48e6;
-  static int slab_planes(const GridDev& g) {
-    if (g.dim != 3 || std::getenv("PDEB200_NO_SLABS") != nullptr) return 0;
-    const double plane = 3.0 * sizeof(T) * (double)g.sxy;  // x, k, b of one plane
-    if (plane * (g.nz - 2) < 2.0 * kSlabBytes) return 0;     // the whole level fits: plain passes
-    const int s = (int)(kSlabBytes / plane) - 3;
-    return s >= 4 ? s : 4;
-  }
-  static dim3 slab_grid(const GridDev& g, int planes) {
-    const dim3 xy((g.nx + kBx - 1) / kBx, (g.ny + kBy - 1) / kBy, 1);
-    const long long xyb = (long long)xy.x * xy.y;
-    long long chunks = (148LL * 9 + xyb - 1) / xyb;
-    if (chunks > planes) chunks = planes;
-    if (chunks < 1) chunks = 1;
-    return dim3(xy.x, xy.y, (unsigned)chunks);
-  }
-  // One sweep by slabs: colours `c0` then `c0 ^ 1`; `zero`: x is taken as
-  // zero by the first colour; `dot`: both colours sum b * (new x) into r.z and
-  // the last launch forms beta.
-  void slab_sweep(Context* ctx, Level& L, const T* b, T* x, int c0, bool zero, const Ctl* ctl, int lvl,
-                  const RedSlot* dot) {
-    const int S = L.slab, kb = 1, ke = L.g.nz - 1;
-    const double plane_dofs = (double)(L.g.nx - 2) * (L.g.ny - 2);
-    const dim3 block = stencil_block();
-    bool first_launch = true;
-    auto pass = [&](int color, int zb, int ze, bool zero_pass, bool last) {
-      if (ze <= zb) return;
-      const dim3 grid = slab_grid(L.g, ze - zb);
-      ProfScope ps(ctx, "rbgs_slab_pass", lvl, plane_dofs * (ze - zb) * (zero_pass ? 1.0 : 2.0) * sizeof(T));
-      if (dot) {
-        if (first_launch)
-          k_rbgs<Coef, T, T, false, true, PostRZPart><<<grid, block, 0, ctx->stream>>>(
-              L.g, L.cf, b, x, color, ctl, *dot, PostRZPart{const_cast<Ctl*>(ctl)}, zb, ze);
-        else if (last)
-          k_rbgs<Coef, T, T, false, true, PostBetaSplit><<<grid, block, 0, ctx->stream>>>(
-              L.g, L.cf, b, x, color, ctl, *dot, PostBetaSplit{const_cast<Ctl*>(ctl)}, zb, ze);
-        else
-          k_rbgs<Coef, T, T, false, true, PostRZAdd><<<grid, block, 0, ctx->stream>>>(
-              L.g, L.cf, b, x, color, ctl, *dot, PostRZAdd{const_cast<Ctl*>(ctl)}, zb, ze);
-      } else if (zero_pass) {
-        k_rbgs<Coef, T, T, true><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, x, color, ctl, RedSlot{}, NoPost{},
-                                                                    zb, ze);
-      } else {
-        k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, x, color, ctl, RedSlot{}, NoPost{}, zb,
-                                                            ze);
-      }
-      ctx->count();
-      first_launch = false;
-    };
-    for (int a = kb; a < ke; a += S) {
-      const int e = std::min(ke, a + S);
-      pass(c0, a, e, zero, false);                             // first colour on [a, e)
-      pass(c0 ^ 1, std::max(kb, a - 1), e - 1, false, false);  // second colour on [a-1, e-1)
-    }
-    pass(c0 ^ 1, ke - 1, ke, false, true);                     // second colour of the last plane
   }
 
   // `sweeps` red-black sweeps starting from `cur` (or from zero); returns the
@@ -749,12 +675,6 @@ struct Hierarchy {
           ProfScope ps(ctx, "zero_fill", lvl, dofs * sizeof(T));
           vfill<T>(ctx, L.g.n, L.xa, T(0), ctl);
         }
-      }
-      if (L.slab > 0) {
-        for (int s = 0; s < sweeps; ++s)
-          slab_sweep(ctx, L, b, cur, first, from_zero && s == 0, ctl, lvl,
-                     (dot_last && s + 1 == sweeps) ? dot_last : nullptr);
-        return cur;
       }
       for (int s = 0; s < sweeps; ++s) {
         for (int half = 0; half < 2; ++half) {
@@ -855,10 +775,6 @@ struct Hierarchy {
     ctx->count();
     if (l == 0 && dot_slot && post > 0 && L.march) {
       // the last sweep also sums r.z (b is r on level 0) and forms beta
-      cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l, dot_slot);
-      dot_done = true;
-    } else if (l == 0 && dot_slot && post > 0 && L.slab > 0) {
-      // the last sweep's slab passes also sum r.z and its last launch forms beta
       cur = sweeps_from(ctx, L, b, cur, post, 1, false, ctl, l, dot_slot);
       dot_done = true;
     } else if (l == 0 && dot_slot && post > 0 && !fused && !L.single_pass) {

@@ -269,24 +269,3 @@ def test_marching_sweep_matches_colour_passes(monkeypatch, which):
     assert ra.status == abi.OK and rb.status == abi.OK
     assert ra.iterations == rb.iterations
     assert rel_l2(a, b) <= 1e-12
-
-
-def test_slab_schedule_matches_whole_grid_passes(monkeypatch):
-    # levels whose x, k and b exceed the L2 budget smooth slab by slab (each
-    # slab's first colour, then the second colour trailing it by one plane);
-    # every node gets the update of the whole-grid passes, so the solve agrees
-    # to rounding (r.z is summed in a different order) at the same iteration count
-    p = synthetic.varcoef_poisson_3d(161, seed=3)
-    opt = default_options(method=abi.MG_PCG, tol=1e-11, tol_mode=abi.TOL_RELATIVE, max_iter=200)
-    a, ra = solver.solve(p, opt)
-    monkeypatch.setenv("PDEB200_NO_SLABS", "1")
-    b, rb = solver.solve(p, opt)
-    assert ra.status == abi.OK and rb.status == abi.OK
-    assert ra.iterations == rb.iterations
-    assert rel_l2(a, b) <= 1e-12
-    # the mixed-precision core (FP32 levels) takes the same schedule
-    monkeypatch.delenv("PDEB200_NO_SLABS")
-    m, rm = solver.solve(p, default_options(method=abi.MG_PCG, tol=1e-10, tol_mode=abi.TOL_RELATIVE, max_iter=200,
-                                            precision=abi.MIXED))
-    assert rm.status == abi.OK and rm.rel_residual <= 1e-10
-    assert rel_l2(m, b) <= 1e-8
