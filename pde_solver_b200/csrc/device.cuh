@@ -45,12 +45,16 @@ struct Stencil {
 
 // Constant coefficients, precomputed on the host with the reference's own
 // expressions (src/backends/cpu/solver.cpp:723-729) so they are bit-identical.
+// Prefetch of the 32-byte sector holding p into L2 (no register result).
+__device__ __forceinline__ void pf_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 struct CoefConst {
   double c, xm, xp, ym, yp, zm, zp;
-  template <typename T>
+  template <typename T, int D = 0>
   __device__ __forceinline__ Stencil<T> at(const GridDev&, long long) const {
     return Stencil<T>{T(c), T(xm), T(xp), T(ym), T(yp), T(zm), T(zp)};
   }
+  __device__ __forceinline__ void prefetch(long long) const {}
 };
 
 template <typename KT>
@@ -72,8 +76,11 @@ struct CoefDivk {
   const KT* k;
   double ihx2, ihy2, ihz2;  // 1/h^2
   double cx, dyc, dzc, e;   // c/(2dx), d/(2dy), dz/(2dz), e
-  template <typename T>
+  __device__ __forceinline__ void prefetch(long long id) const { pf_l2(k + id); }
+  // D: the grid dimension when the caller knows it at compile time, else 0
+  template <typename T, int D = 0>
   __device__ __forceinline__ Stencil<T> at(const GridDev& g, long long id) const {
+    const bool d3 = D ? D == 3 : g.dim == 3;
     if constexpr (sizeof(T) == 4) {
       // FP32 stencils (preconditioner levels of the precision form) in FP32
       const float kc = float(load_k(k, id));
@@ -86,7 +93,7 @@ struct CoefDivk {
       s.ym = T(-kym * fy - float(dyc));
       s.yp = T(-kyp * fy + float(dyc));
       float c = (kxm + kxp) * fx + (kym + kyp) * fy;
-      if (g.dim == 3) {
+      if (d3) {
         const float fz = float(ihz2);
         const float kzm = 0.5f * (kc + float(load_k(k, id - g.sxy))), kzp = 0.5f * (kc + float(load_k(k, id + g.sxy)));
         s.zm = T(-kzm * fz - float(dzc));
@@ -107,7 +114,7 @@ struct CoefDivk {
     s.ym = T(-kym * ihy2 - dyc);
     s.yp = T(-kyp * ihy2 + dyc);
     double c = (kxm + kxp) * ihx2 + (kym + kyp) * ihy2;
-    if (g.dim == 3) {
+    if (d3) {
       const double kzm = 0.5 * (kc + load_k(k, id - g.sxy)), kzp = 0.5 * (kc + load_k(k, id + g.sxy));
       s.zm = T(-kzm * ihz2 - dzc);
       s.zp = T(-kzp * ihz2 + dzc);
@@ -126,8 +133,10 @@ struct CoefNodal {
   const double* nodal;
   long long n;
   double dx2, dy2, dz2, tdx, tdy, tdz;  // dx*dx, ..., 2*dx, ...
-  template <typename T>
+  __device__ __forceinline__ void prefetch(long long) const {}
+  template <typename T, int D = 0>
   __device__ __forceinline__ Stencil<T> at(const GridDev& g, long long id) const {
+    const bool d3 = D ? D == 3 : g.dim == 3;
     const double a = __ldg(nodal + id), b = __ldg(nodal + n + id);
     const double c = __ldg(nodal + 3 * n + id), d = __ldg(nodal + 4 * n + id), e = __ldg(nodal + 6 * n + id);
     const double ax = __ddiv_rn(a, dx2), by = __ddiv_rn(b, dy2);
@@ -137,7 +146,7 @@ struct CoefNodal {
     s.xm = T(__dsub_rn(ax, cx));
     s.yp = T(__dadd_rn(by, dyc));
     s.ym = T(__dsub_rn(by, dyc));
-    if (g.dim == 3) {
+    if (d3) {
       const double az = __ldg(nodal + 2 * n + id), dzv = __ldg(nodal + 5 * n + id);
       const double cz = __ddiv_rn(az, dz2), dzc = __ddiv_rn(dzv, tdz);
       s.zp = T(__dadd_rn(cz, dzc));
@@ -154,9 +163,10 @@ struct CoefNodal {
 // Folding of the boundary closure of face-adjacent interior nodes:
 // diag += w_face * c1, the face term is dropped, and (optionally) w_face*c0
 // is accumulated for the right-hand side.
-template <typename T>
+template <typename T, int D = 0>
 __device__ __forceinline__ void fold_faces(const GridDev& g, int i, int j, int k, Stencil<T>& s,
                                            double* bshift) {
+  const bool d3 = D ? D == 3 : g.dim == 3;
   double sh = 0.0;
   if (i == 1) {
     const FaceDev& f = g.face[kLeft];
@@ -186,7 +196,7 @@ __device__ __forceinline__ void fold_faces(const GridDev& g, int i, int j, int k
     sh += double(s.yp) * f.c0.at(loc);
     s.yp = T(0);
   }
-  if (g.dim == 3) {
+  if (d3) {
     if (k == 1) {
       const FaceDev& f = g.face[kFront];
       const int loc = i + g.nx * j;

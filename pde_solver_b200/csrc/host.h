@@ -7,6 +7,7 @@
 
 #include <memory>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -110,6 +111,7 @@ struct Context {
   double* d_redout = nullptr;
   size_t max_blocks = 0;
   int num_sms = 148;
+  bool pdl = true;  // launch_dep launches carry programmatic stream serialization
   std::string name;
   std::mutex mu;
   long long launches = 0;
@@ -239,6 +241,28 @@ inline int vec_blocks(long long n, const Context* ctx) {
   long long b = (n + 255) / 256;
   long long cap = (long long)ctx->num_sms * 8;
   return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+// Launch of a kernel that calls ctl_skip() before its first memory access,
+// with programmatic stream serialization when ctx->pdl is set: the launch may
+// be scheduled while the previous kernel of the stream drains, and waits in
+// ctl_skip until that kernel has completed. Inside a captured graph this
+// becomes a programmatic edge. The arguments are those of the kernel in full
+// (no defaulted parameters).
+template <typename... KArgs, typename... Args>
+inline void launch_dep(const Context* ctx, dim3 grid, dim3 block, size_t smem, void (*kern)(KArgs...),
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = ctx->pdl ? 1 : 0;
+  PDEB_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
 }
 
 // Dispatch on the coefficient form of a DevProblem: fn(coef) with the concrete type.

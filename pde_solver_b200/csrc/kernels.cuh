@@ -38,7 +38,22 @@ struct Ctl {
   double aux[8];
 };
 
-__device__ __forceinline__ bool ctl_skip(const Ctl* c) { return c && *((volatile const int*)&c->done); }
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization (launch_dep on the host) may be scheduled while the previous
+// kernel of the stream is still running. grid_dep_wait() returns once that
+// kernel has completed and its writes are visible (at once for an ordinary
+// launch); grid_dep_release() lets the next such launch be scheduled. Every
+// kernel calls both in ctl_skip, before its first memory access, so at most
+// one kernel is scheduled ahead and it touches no memory until its
+// predecessor is done: the results are those of plain stream order.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+__device__ __forceinline__ bool ctl_skip(const Ctl* c) {
+  grid_dep_wait();
+  grid_dep_release();
+  return c && *((volatile const int*)&c->done);
+}
 __device__ __forceinline__ bool ctl_stopped(const Ctl* c) {
   return c && (*((volatile const int*)&c->done) || *((volatile const int*)&c->stop));
 }
@@ -55,6 +70,83 @@ __device__ __forceinline__ void column_range(const GridDev& g, int& k0, int& k1)
 
 // ------------------------------------------------------------ folded apply
 
+// Planes ahead of the current trip that the apply and the residual prefetch
+// into L2 (x, k and b of two planes per trip): at 257^3 the apply goes from
+// 141 to 116 us and the residual from 141 to 127 us; 2, 6 and 8 planes ahead
+// are slower. The colour pass is slower with any prefetch distance.
+constexpr int kPfPlanes = 4;
+
+// The columns of one thread of k_apply_folded / k_residual_folded (RES: r = b
+// - A x, else y = A x). D is the grid dimension: the kernels branch on it
+// once, and the stencil helpers take it as a constant (with the prefetch,
+// 257^3 apply 116 -> 105 us, residual 127 -> 121 us). acc sums x*y (apply) or
+// r*r (residual) when NV > 0.
+template <int D, bool RES, int NV, class Coef, typename T, typename TB>
+__device__ __forceinline__ void stencil_columns(const GridDev& g, const Coef& cf, const T* __restrict__ x,
+                                                const TB* __restrict__ b, T* __restrict__ y, double& acc) {
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) return;
+  long long id = ((long long)k0 * g.ny + j) * g.nx + i;
+  T zm = D == 3 ? x[id - g.sxy] : T(0);
+  T zc = x[id];
+  int k = k0;
+  // two planes per trip, all loads before the stores (with one plane per
+  // trip the kernels are latency-bound)
+  for (; k + 1 < k1; k += 2, id += 2 * g.sxy) {
+    if (k + kPfPlanes + 1 < g.nz) {
+      const long long a = id + kPfPlanes * g.sxy;
+      pf_l2(x + a);
+      pf_l2(x + a + g.sxy);
+      cf.prefetch(a);
+      cf.prefetch(a + g.sxy);
+      if constexpr (RES) {
+        pf_l2(b + a);
+        pf_l2(b + a + g.sxy);
+      }
+    }
+    const long long id2 = id + g.sxy;
+    const T z1 = x[id2];
+    const T z2 = x[id2 + g.sxy];
+    const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
+    const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
+    T b1 = T(0), b2 = T(0);
+    if constexpr (RES) {
+      b1 = T(b[id]);
+      b2 = T(b[id2]);
+    }
+    Stencil<T> s = cf.template at<T, D>(g, id);
+    Stencil<T> s2 = cf.template at<T, D>(g, id2);
+    fold_faces<T, D>(g, i, j, k, s, nullptr);
+    fold_faces<T, D>(g, i, j, k + 1, s2, nullptr);
+    const T a1 = s.c * zc + nb_sum<T>(s, xp1, xm1, yp1, ym1, z1, zm, D);
+    const T a2 = s2.c * z1 + nb_sum<T>(s2, xp2, xm2, yp2, ym2, z2, zc, D);
+    const T v = RES ? b1 - a1 : a1;
+    const T v2 = RES ? b2 - a2 : a2;
+    y[id] = v;
+    y[id2] = v2;
+    if constexpr (NV > 0) {
+      acc += RES ? double(v) * double(v) : double(zc) * double(v);
+      acc += RES ? double(v2) * double(v2) : double(z1) * double(v2);
+    }
+    zm = z1;
+    zc = z2;
+  }
+  for (; k < k1; ++k, id += g.sxy) {
+    const T zp = D == 3 ? x[id + g.sxy] : T(0);
+    Stencil<T> s = cf.template at<T, D>(g, id);
+    fold_faces<T, D>(g, i, j, k, s, nullptr);
+    const T a = s.c * zc + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, D);
+    const T v = RES ? T(b[id]) - a : a;
+    y[id] = v;
+    if constexpr (NV > 0) acc += RES ? double(v) * double(v) : double(zc) * double(v);
+    zm = zc;
+    zc = zp;
+  }
+}
+
 // y = A_fold x on interior nodes (boundary rows of y untouched), with optional
 // fused sum(w * y) (w = x for p.Ap).
 template <class Coef, typename T, int NV, class Post>
@@ -62,106 +154,27 @@ __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, c
                                                            T* __restrict__ y, RedSlot slot, Post post,
                                                            const Ctl* ctl) {
   if (ctl_skip(ctl)) return;
-  const int i = blockIdx.x * kBx + threadIdx.x;
-  const int j = blockIdx.y * kBy + threadIdx.y;
-  int k0, k1;
-  column_range(g, k0, k1);
   double acc[(NV > 0 ? NV : 1)] = {0.0};
-  const bool active = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
-  if (active && k0 < k1) {
-    long long id = ((long long)k0 * g.ny + j) * g.nx + i;
-    T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-    T zc = x[id];
-    int k = k0;
-    // two planes per trip, all loads before the stores (see k_residual_folded)
-    for (; k + 1 < k1; k += 2, id += 2 * g.sxy) {
-      const long long id2 = id + g.sxy;
-      const T z1 = x[id2];
-      const T z2 = x[id2 + g.sxy];
-      const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
-      const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
-      Stencil<T> s = cf.template at<T>(g, id);
-      Stencil<T> s2 = cf.template at<T>(g, id2);
-      fold_faces<T>(g, i, j, k, s, nullptr);
-      fold_faces<T>(g, i, j, k + 1, s2, nullptr);
-      const T v = s.c * zc + nb_sum<T>(s, xp1, xm1, yp1, ym1, z1, zm, g.dim);
-      const T v2 = s2.c * z1 + nb_sum<T>(s2, xp2, xm2, yp2, ym2, z2, zc, g.dim);
-      y[id] = v;
-      y[id2] = v2;
-      if constexpr (NV > 0) {
-        acc[0] += double(zc) * double(v);
-        acc[0] += double(z1) * double(v2);
-      }
-      zm = z1;
-      zc = z2;
-    }
-    for (; k < k1; ++k, id += g.sxy) {
-      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
-      Stencil<T> s = cf.template at<T>(g, id);
-      fold_faces<T>(g, i, j, k, s, nullptr);
-      const T v = s.c * zc + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim);
-      y[id] = v;
-      if constexpr (NV > 0) acc[0] += double(zc) * double(v);
-      zm = zc;
-      zc = zp;
-    }
-  }
+  if (g.dim == 3)
+    stencil_columns<3, false, NV, Coef, T, T>(g, cf, x, nullptr, y, acc[0]);
+  else
+    stencil_columns<2, false, NV, Coef, T, T>(g, cf, x, nullptr, y, acc[0]);
   if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
 }
 
 // r = b - A_fold x on interior nodes, optional fused |r|^2. Capped at 64
-// registers (4 blocks/SM; 16 bytes spill): 138 -> 133 us at 257^3. The same cap
-// on k_apply_folded spills 88 bytes and is slower.
+// registers (4 blocks/SM, some spill): at 257^3 121 us, against 124 us with
+// 3 blocks/SM.
 template <class Coef, typename T, typename TB, int NV, class Post>
 __global__ void __launch_bounds__(kBx* kBy, 4) k_residual_folded(GridDev g, Coef cf, const T* __restrict__ x,
                                                               const TB* __restrict__ b, T* __restrict__ r,
                                                               RedSlot slot, Post post, const Ctl* ctl) {
   if (ctl_skip(ctl)) return;
-  const int i = blockIdx.x * kBx + threadIdx.x;
-  const int j = blockIdx.y * kBy + threadIdx.y;
-  int k0, k1;
-  column_range(g, k0, k1);
   double acc[(NV > 0 ? NV : 1)] = {0.0};
-  const bool active = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
-  if (active && k0 < k1) {
-    long long id = ((long long)k0 * g.ny + j) * g.nx + i;
-    T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-    T zc = x[id];
-    int k = k0;
-    // two planes per trip, all loads before the stores (see k_apply_folded)
-    for (; k + 1 < k1; k += 2, id += 2 * g.sxy) {
-      const long long id2 = id + g.sxy;
-      const T z1 = x[id2];
-      const T z2 = x[id2 + g.sxy];
-      const T xp1 = x[id + 1], xm1 = x[id - 1], yp1 = x[id + g.nx], ym1 = x[id - g.nx];
-      const T xp2 = x[id2 + 1], xm2 = x[id2 - 1], yp2 = x[id2 + g.nx], ym2 = x[id2 - g.nx];
-      const T b1 = T(b[id]), b2 = T(b[id2]);
-      Stencil<T> s = cf.template at<T>(g, id);
-      Stencil<T> s2 = cf.template at<T>(g, id2);
-      fold_faces<T>(g, i, j, k, s, nullptr);
-      fold_faces<T>(g, i, j, k + 1, s2, nullptr);
-      const T v = b1 - (s.c * zc + nb_sum<T>(s, xp1, xm1, yp1, ym1, z1, zm, g.dim));
-      const T v2 = b2 - (s2.c * z1 + nb_sum<T>(s2, xp2, xm2, yp2, ym2, z2, zc, g.dim));
-      r[id] = v;
-      r[id2] = v2;
-      if constexpr (NV > 0) {
-        acc[0] += double(v) * double(v);
-        acc[0] += double(v2) * double(v2);
-      }
-      zm = z1;
-      zc = z2;
-    }
-    for (; k < k1; ++k, id += g.sxy) {
-      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
-      Stencil<T> s = cf.template at<T>(g, id);
-      fold_faces<T>(g, i, j, k, s, nullptr);
-      const T v = T(b[id]) - (s.c * zc + nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim));
-      r[id] = v;
-      if constexpr (NV > 0) acc[0] += double(v) * double(v);
-      zm = zc;
-      zc = zp;
-    }
-  }
+  if (g.dim == 3)
+    stencil_columns<3, true, NV, Coef, T, TB>(g, cf, x, b, r, acc[0]);
+  else
+    stencil_columns<2, true, NV, Coef, T, TB>(g, cf, x, b, r, acc[0]);
   if constexpr (NV > 0) grid_reduce<(NV > 0 ? NV : 1), false>(acc, slot, post);
 }
 
@@ -183,6 +196,69 @@ __global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, con
   }
 }
 
+// The columns of one thread of a colour pass. D is the grid dimension: the
+// kernel branches on it once, so the field loads of the 3D form are not
+// predicated and are all issued before the stores (with run-time dimension
+// tests on them the 257^3 pass takes 120 instead of 107 us). HD is the
+// dimension handed to the stencil helpers (0: their run-time test); the 3D
+// form keeps the run-time test there, which measured faster than the
+// constant (118 us).
+template <int D, int HD, class Coef, typename T, typename TB, bool ZERO, bool DOT>
+__device__ __forceinline__ void rbgs_columns(const GridDev& g, const Coef& cf, const TB* __restrict__ b,
+                                             T* __restrict__ x, int color, double& acc) {
+  const int i = blockIdx.x * kBx + threadIdx.x;
+  const int j = blockIdx.y * kBy + threadIdx.y;
+  int k0, k1;
+  column_range(g, k0, k1);
+  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) return;
+  const int nd = HD ? HD : g.dim;
+  int k = k0 + ((i + j + k0 + color) & 1);
+  auto ld = [&](long long q) -> T {
+    if constexpr (ZERO) return T(0);
+    return x[q];
+  };
+  // nodes k and k+2 of one colour per trip: neither reads the other (their
+  // neighbours are all of the other colour), so both nodes' loads are issued
+  // before either store
+  for (; k + 2 < k1; k += 4) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i, id2 = id + 2 * g.sxy;
+    Stencil<T> s = cf.template at<T, HD>(g, id);
+    Stencil<T> s2 = cf.template at<T, HD>(g, id2);
+    const T b1 = T(b[id]), b2 = T(b[id2]);
+    const T zm = D == 3 ? ld(id - g.sxy) : T(0);
+    const T mid = D == 3 ? ld(id + g.sxy) : T(0);  // zp of node k, zm of node k+2
+    const T zp2 = D == 3 ? ld(id2 + g.sxy) : T(0);
+    const T xp1 = ld(id + 1), xm1 = ld(id - 1), yp1 = ld(id + g.nx), ym1 = ld(id - g.nx);
+    const T xp2 = ld(id2 + 1), xm2 = ld(id2 - 1), yp2 = ld(id2 + g.nx), ym2 = ld(id2 - g.nx);
+    fold_faces<T, HD>(g, i, j, k, s, nullptr);
+    fold_faces<T, HD>(g, i, j, k + 2, s2, nullptr);
+    const T v1 = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, nd)) / s.c;
+    const T v2 = (b2 - nb_sum<T>(s2, xp2, xm2, yp2, ym2, zp2, mid, nd)) / s2.c;
+    x[id] = v1;
+    x[id2] = v2;
+    if constexpr (DOT) {
+      acc += double(b1) * double(v1);
+      acc += double(b2) * double(v2);
+    }
+  }
+  for (; k < k1; k += 2) {
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    Stencil<T> s = cf.template at<T, HD>(g, id);
+    fold_faces<T, HD>(g, i, j, k, s, nullptr);
+    if constexpr (ZERO) {
+      const T z0 = T(0);
+      x[id] = (T(b[id]) - nb_sum<T>(s, z0, z0, z0, z0, z0, z0, nd)) / s.c;
+    } else {
+      const T zp = D == 3 ? x[id + g.sxy] : T(0);
+      const T zm = D == 3 ? x[id - g.sxy] : T(0);
+      const T bv = T(b[id]);
+      const T v = (bv - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, nd)) / s.c;
+      x[id] = v;
+      if constexpr (DOT) acc += double(bv) * double(v);
+    }
+  }
+}
+
 // One red-black Gauss-Seidel colour pass on the folded operator; colour of
 // (i,j,k) is (i+j+k)&1. The updated colour only reads the other colour, so a
 // pass is race free.
@@ -195,65 +271,16 @@ __global__ void __launch_bounds__(kBx* kBy) k_folded_rhs(GridDev g, Coef cf, con
 // and handed to `post` (the last two passes of a V-cycle's finest level give
 // r.z of preconditioned CG, since b is r there).
 template <class Coef, typename T, typename TB, bool ZERO = false, bool DOT = false, class Post = NoPost>
-__global__ void __launch_bounds__(kBx* kBy) k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x,
-                                                   int color, const Ctl* ctl, RedSlot slot = RedSlot{},
-                                                   Post post = Post{}) {
+__global__ void __launch_bounds__(kBx* kBy, ZERO ? 4 : 3)
+    k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x, int color, const Ctl* ctl,
+           RedSlot slot = RedSlot{}, Post post = Post{}) {
   if (ctl_skip(ctl)) return;
-  const int i = blockIdx.x * kBx + threadIdx.x;
-  const int j = blockIdx.y * kBy + threadIdx.y;
-  int k0, k1;
-  column_range(g, k0, k1);
-  double acc[1] = {0.0};
   // with DOT every thread reaches the block reduction at the end
-  if (!(i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) || k0 >= k1) {
-    if constexpr (!DOT) return;
-    k1 = k0;  // no nodes: both loops below are empty
-  }
-  int k = k0 + ((i + j + k0 + color) & 1);
-  // nodes k and k+2 of one colour per trip: neither reads the other (their
-  // neighbours are all of the other colour), so both nodes' loads are issued
-  // before either store
-  for (; k + 2 < k1; k += 4) {
-    const long long id = ((long long)k * g.ny + j) * g.nx + i, id2 = id + 2 * g.sxy;
-    Stencil<T> s = cf.template at<T>(g, id);
-    Stencil<T> s2 = cf.template at<T>(g, id2);
-    const T b1 = T(b[id]), b2 = T(b[id2]);
-    auto ld = [&](long long q) -> T {
-      if constexpr (ZERO) return T(0);
-      return x[q];
-    };
-    const T zm = g.dim == 3 ? ld(id - g.sxy) : T(0);
-    const T mid = g.dim == 3 ? ld(id + g.sxy) : T(0);  // zp of node k, zm of node k+2
-    const T zp2 = g.dim == 3 ? ld(id2 + g.sxy) : T(0);
-    const T xp1 = ld(id + 1), xm1 = ld(id - 1), yp1 = ld(id + g.nx), ym1 = ld(id - g.nx);
-    const T xp2 = ld(id2 + 1), xm2 = ld(id2 - 1), yp2 = ld(id2 + g.nx), ym2 = ld(id2 - g.nx);
-    fold_faces<T>(g, i, j, k, s, nullptr);
-    fold_faces<T>(g, i, j, k + 2, s2, nullptr);
-    const T v1 = (b1 - nb_sum<T>(s, xp1, xm1, yp1, ym1, mid, zm, g.dim)) / s.c;
-    const T v2 = (b2 - nb_sum<T>(s2, xp2, xm2, yp2, ym2, zp2, mid, g.dim)) / s2.c;
-    x[id] = v1;
-    x[id2] = v2;
-    if constexpr (DOT) {
-      acc[0] += double(b1) * double(v1);
-      acc[0] += double(b2) * double(v2);
-    }
-  }
-  for (; k < k1; k += 2) {
-    const long long id = ((long long)k * g.ny + j) * g.nx + i;
-    Stencil<T> s = cf.template at<T>(g, id);
-    fold_faces<T>(g, i, j, k, s, nullptr);
-    if constexpr (ZERO) {
-      const T z0 = T(0);
-      x[id] = (T(b[id]) - nb_sum<T>(s, z0, z0, z0, z0, z0, z0, g.dim)) / s.c;
-    } else {
-      const T zp = g.dim == 3 ? x[id + g.sxy] : T(0);
-      const T zm = g.dim == 3 ? x[id - g.sxy] : T(0);
-      const T bv = T(b[id]);
-      const T v = (bv - nb_sum<T>(s, x[id + 1], x[id - 1], x[id + g.nx], x[id - g.nx], zp, zm, g.dim)) / s.c;
-      x[id] = v;
-      if constexpr (DOT) acc[0] += double(bv) * double(v);
-    }
-  }
+  double acc[1] = {0.0};
+  if (g.dim == 3)
+    rbgs_columns<3, 0, Coef, T, TB, ZERO, DOT>(g, cf, b, x, color, acc[0]);
+  else
+    rbgs_columns<2, 2, Coef, T, TB, ZERO, DOT>(g, cf, b, x, color, acc[0]);
   if constexpr (DOT) grid_reduce<1, false>(acc, slot, post);
 }
 

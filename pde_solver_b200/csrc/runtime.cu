@@ -44,6 +44,7 @@ void init_context(Context* c, int dev) {
   PDEB_CUDA(cudaGetDeviceProperties(&prop, dev));
   c->name = prop.name;
   c->num_sms = prop.multiProcessorCount;
+  c->pdl = std::getenv("PDEB200_NO_PDL") == nullptr;
   PDEB_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
   c->stream = c->own_stream;
   PDEB_CUDA(cudaEventCreate(&c->ev0));

@@ -161,24 +161,25 @@ pdeb200_status mg_pcg(Context* ctx, DevProblem& P, const Coef& cf, const pdeb200
   auto iterate = [&](int) {
     {
       ProfScope ps(ctx, "apply_dot", 0, dofs * 24.0);
-      k_apply_folded<Coef, double, 1, PostAlpha><<<grid, block, 0, ctx->stream>>>(g, cf, p, q, ctx->slot(),
-                                                                                   PostAlpha{ctx->d_ctl}, ctx->d_ctl);
+      launch_dep(ctx, grid, block, 0, k_apply_folded<Coef, double, 1, PostAlpha>, g, cf, (const double*)p, q,
+                 ctx->slot(), PostAlpha{ctx->d_ctl}, (const Ctl*)ctx->d_ctl);
     }
     {
       ProfScope ps(ctx, "cg_update_xr", 0, dofs * 48.0);
-      k_cg_xr<double, PostRRRel><<<nb, 256, 0, ctx->stream>>>(n, d_x, r, p, q, ctx->slot(), PostRRRel{ctx->d_ctl},
-                                                              ctx->d_ctl);
+      launch_dep(ctx, dim3(nb), dim3(256), 0, k_cg_xr<double, PostRRRel>, n, d_x, r, (const double*)p,
+                 (const double*)q, ctx->slot(), PostRRRel{ctx->d_ctl}, ctx->d_ctl);
     }
     ctx->count(2);
     // beta from r.z: summed by the preconditioner's last two colour passes
     // when it can, else by a separate dot
     if (!H.vcycle_dot(ctx, r, ctx->d_ctl, ctx->slot())) {
       ProfScope ps(ctx, "dot", 0, dofs * 16.0);
-      k_dot<double, PostBeta><<<nb, 256, 0, ctx->stream>>>(n, r, z, ctx->slot(), PostBeta{ctx->d_ctl}, ctx->d_ctl);
+      launch_dep(ctx, dim3(nb), dim3(256), 0, k_dot<double, PostBeta>, n, (const double*)r, (const double*)z,
+                 ctx->slot(), PostBeta{ctx->d_ctl}, (const Ctl*)ctx->d_ctl);
     }
     {
       ProfScope ps(ctx, "cg_update_p", 0, dofs * 24.0);
-      k_cg_p<double><<<nb, 256, 0, ctx->stream>>>(n, p, z, ctx->d_ctl, 0);
+      launch_dep(ctx, dim3(nb), dim3(256), 0, k_cg_p<double>, n, p, (const double*)z, (const Ctl*)ctx->d_ctl, 0);
     }
     ctx->count(2);
   };

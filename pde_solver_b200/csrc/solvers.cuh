@@ -681,11 +681,13 @@ struct Hierarchy {
           if (from_zero && s == 0 && half == 0) {
             // b and the written half of x: 8 B per DOF in FP64
             ProfScope ps(ctx, "rbgs_zero_pass", lvl, dofs * sizeof(T));
-            k_rbgs<Coef, T, T, true><<<zgrid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first, ctl);
+            launch_dep(ctx, zgrid, block, 0, k_rbgs<Coef, T, T, true>, L.g, L.cf, b, cur, first, ctl, RedSlot{},
+                       NoPost{});
             continue;
           }
           ProfScope ps(ctx, "rbgs_color_pass", lvl, dofs * 2.0 * sizeof(T));
-          k_rbgs<Coef, T, T><<<grid, block, 0, ctx->stream>>>(L.g, L.cf, b, cur, first ^ half, ctl);
+          launch_dep(ctx, grid, block, 0, k_rbgs<Coef, T, T>, L.g, L.cf, b, cur, first ^ half, ctl, RedSlot{},
+                     NoPost{});
         }
         ctx->count(2);
       }
@@ -712,8 +714,8 @@ struct Hierarchy {
     const double dofs = interior_dofs(L.g);
     if (l == tail_l0) {
       ProfScope ps(ctx, "tail_vcycle", l, 0.0);
-      k_tail_vcycle<Coef, T><<<1, kTailThreads, 0, ctx->stream>>>(d_tail, (int)levels.size() - l, b, pre, post,
-                                                                    coarse_iters, needs_fold ? 1 : 0, ctl);
+      launch_dep(ctx, dim3(1), dim3(kTailThreads), 0, k_tail_vcycle<Coef, T>, (const TailLevel<Coef, T>*)d_tail,
+                 (int)levels.size() - l, b, pre, post, coarse_iters, needs_fold ? 1 : 0, ctl);
       ctx->count();
       return;
     }
@@ -736,8 +738,8 @@ struct Hierarchy {
     }
     {
       ProfScope ps(ctx, "residual", l, dofs * 4.0 * sizeof(T));
-      k_residual_folded<Coef, T, T, 0, NoPost><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(
-          L.g, L.cf, cur, b, L.r, RedSlot{}, NoPost{}, ctl);
+      launch_dep(ctx, stencil_grid_auto(L.g), stencil_block(), 0, k_residual_folded<Coef, T, T, 0, NoPost>, L.g,
+                 L.cf, (const T*)cur, b, L.r, RedSlot{}, NoPost{}, ctl);
     }
     Level& C = levels[l + 1];
     {
@@ -748,16 +750,17 @@ struct Hierarchy {
         // take one plane per thread (latency rather than bytes). The result
         // does not depend on the chunking: a chunk's first plane sum is
         // recomputed with the same arithmetic as a carried one.
-        k_restrict_march<T, T><<<stencil_grid_full(C.g, C.g.n > (1LL << 20) ? 4 : 1), stencil_block(), 0,
-                                 ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+        launch_dep(ctx, stencil_grid_full(C.g, C.g.n > (1LL << 20) ? 4 : 1), stencil_block(), 0,
+                   k_restrict_march<T, T>, L.g, C.g, (const T*)L.r, C.b, ctl);
       else
-        k_restrict_fw<T, T><<<stencil_grid_full(C.g, 1), stencil_block(), 0, ctx->stream>>>(L.g, C.g, L.r, C.b, ctl);
+        launch_dep(ctx, stencil_grid_full(C.g, 1), stencil_block(), 0, k_restrict_fw<T, T>, L.g, C.g, (const T*)L.r,
+                   C.b, ctl);
     }
     if (needs_fold) {
       ProfScope ps(ctx, "restrict_fold", l, 0.0);
       const FoldLayers lay = fold_layers(C.g);
       const int blocks = (int)std::max<long long>(1, std::min<long long>((lay.start[6] + 255) / 256, 148LL * 16));
-      k_restrict_fold_faces<T><<<blocks, 256, 0, ctx->stream>>>(C.g, lay, C.b, ctl);
+      launch_dep(ctx, dim3(blocks), dim3(256), 0, k_restrict_fold_faces<T>, C.g, lay, C.b, ctl);
       ctx->count();
     }
     ctx->count(2);
@@ -767,10 +770,11 @@ struct Hierarchy {
       if (z_nested(L.g, C.g))
         // 148*24 target blocks (12 z chunks at 257^3): 101.7 -> 97 us against
         // 148*16; 148*12 and 148*40 are slower
-        k_prolong_march<T, T><<<stencil_grid_auto(L.g, 148 * 24), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out,
-                                                                                                    cur, ctl);
+        launch_dep(ctx, stencil_grid_auto(L.g, 148 * 24), stencil_block(), 0, k_prolong_march<T, T>, L.g, C.g,
+                   (const T*)C.out, cur, ctl);
       else
-        k_prolong_add<T, T><<<stencil_grid_auto(L.g), stencil_block(), 0, ctx->stream>>>(L.g, C.g, C.out, cur, ctl);
+        launch_dep(ctx, stencil_grid_auto(L.g), stencil_block(), 0, k_prolong_add<T, T>, L.g, C.g, (const T*)C.out,
+                   cur, ctl);
     }
     ctx->count();
     if (l == 0 && dot_slot && post > 0 && L.march) {
@@ -783,13 +787,13 @@ struct Hierarchy {
       const dim3 grid = rbgs_grid(L.g), block = stencil_block();
       {
         ProfScope ps(ctx, "rbgs_color_pass", l, dofs * 2.0 * sizeof(T));
-        k_rbgs<Coef, T, T, false, true, PostRZPart><<<grid, block, 0, ctx->stream>>>(
-            L.g, L.cf, b, cur, 1, ctl, *dot_slot, PostRZPart{const_cast<Ctl*>(ctl)});
+        launch_dep(ctx, grid, block, 0, k_rbgs<Coef, T, T, false, true, PostRZPart>, L.g, L.cf, b, cur, 1, ctl,
+                   *dot_slot, PostRZPart{const_cast<Ctl*>(ctl)});
       }
       {
         ProfScope ps(ctx, "rbgs_color_pass", l, dofs * 2.0 * sizeof(T));
-        k_rbgs<Coef, T, T, false, true, PostBetaSplit><<<grid, block, 0, ctx->stream>>>(
-            L.g, L.cf, b, cur, 0, ctl, *dot_slot, PostBetaSplit{const_cast<Ctl*>(ctl)});
+        launch_dep(ctx, grid, block, 0, k_rbgs<Coef, T, T, false, true, PostBetaSplit>, L.g, L.cf, b, cur, 0, ctl,
+                   *dot_slot, PostBetaSplit{const_cast<Ctl*>(ctl)});
       }
       ctx->count(2);
       dot_done = true;
