@@ -243,10 +243,10 @@ inline int vec_blocks(long long n, const Context* ctx) {
   return (int)(b < cap ? (b > 0 ? b : 1) : cap);
 }
 
-// Launch of a kernel that calls ctl_skip() before its first memory access,
+// Launch of a kernel that calls ctl_skip_dep() before its first memory access,
 // with programmatic stream serialization when ctx->pdl is set: the launch may
 // be scheduled while the previous kernel of the stream drains, and waits in
-// ctl_skip until that kernel has completed. Inside a captured graph this
+// ctl_skip_dep until that kernel has completed. Inside a captured graph this
 // becomes a programmatic edge. The arguments are those of the kernel in full
 // (no defaulted parameters).
 template <typename... KArgs, typename... Args>

@@ -38,21 +38,24 @@ struct Ctl {
   double aux[8];
 };
 
+__device__ __forceinline__ bool ctl_skip(const Ctl* c) { return c && *((volatile const int*)&c->done); }
+
 // Programmatic dependent launch: a kernel launched with programmatic stream
 // serialization (launch_dep on the host) may be scheduled while the previous
 // kernel of the stream is still running. grid_dep_wait() returns once that
 // kernel has completed and its writes are visible (at once for an ordinary
-// launch); grid_dep_release() lets the next such launch be scheduled. Every
-// kernel calls both in ctl_skip, before its first memory access, so at most
-// one kernel is scheduled ahead and it touches no memory until its
-// predecessor is done: the results are those of plain stream order.
+// launch); grid_dep_release() lets the next such launch be scheduled. The
+// kernels launch_dep launches call both through ctl_skip_dep, before their
+// first memory access, so at most one kernel is scheduled ahead and it
+// touches no memory until its predecessor is done: the results are those of
+// plain stream order.
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-__device__ __forceinline__ bool ctl_skip(const Ctl* c) {
+__device__ __forceinline__ bool ctl_skip_dep(const Ctl* c) {
   grid_dep_wait();
   grid_dep_release();
-  return c && *((volatile const int*)&c->done);
+  return ctl_skip(c);
 }
 __device__ __forceinline__ bool ctl_stopped(const Ctl* c) {
   return c && (*((volatile const int*)&c->done) || *((volatile const int*)&c->stop));
@@ -153,7 +156,7 @@ template <class Coef, typename T, int NV, class Post>
 __global__ void __launch_bounds__(kBx* kBy) k_apply_folded(GridDev g, Coef cf, const T* __restrict__ x,
                                                            T* __restrict__ y, RedSlot slot, Post post,
                                                            const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   double acc[(NV > 0 ? NV : 1)] = {0.0};
   if (g.dim == 3)
     stencil_columns<3, false, NV, Coef, T, T>(g, cf, x, nullptr, y, acc[0]);
@@ -169,7 +172,7 @@ template <class Coef, typename T, typename TB, int NV, class Post>
 __global__ void __launch_bounds__(kBx* kBy, 4) k_residual_folded(GridDev g, Coef cf, const T* __restrict__ x,
                                                               const TB* __restrict__ b, T* __restrict__ r,
                                                               RedSlot slot, Post post, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   double acc[(NV > 0 ? NV : 1)] = {0.0};
   if (g.dim == 3)
     stencil_columns<3, true, NV, Coef, T, TB>(g, cf, x, b, r, acc[0]);
@@ -274,7 +277,7 @@ template <class Coef, typename T, typename TB, bool ZERO = false, bool DOT = fal
 __global__ void __launch_bounds__(kBx* kBy, ZERO ? 4 : 3)
     k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x, int color, const Ctl* ctl,
            RedSlot slot = RedSlot{}, Post post = Post{}) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   // with DOT every thread reaches the block reduction at the end
   double acc[1] = {0.0};
   if (g.dim == 3)
@@ -637,7 +640,7 @@ __device__ __forceinline__ long long gstride() { return (long long)gridDim.x * b
 template <typename T, class Post>
 __global__ void k_cg_xr(long long n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
                         const T* __restrict__ q, RedSlot slot, Post post, Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const double a = ctl->alpha;
   double acc[1] = {0.0};
   for (long long t = gtid(); t < n; t += gstride()) {
@@ -652,7 +655,7 @@ __global__ void k_cg_xr(long long n, T* __restrict__ x, T* __restrict__ r, const
 // p = z + beta p (beta = ctl->beta; first iteration: p = z)
 template <typename T>
 __global__ void k_cg_p(long long n, T* __restrict__ p, const T* __restrict__ z, const Ctl* ctl, int first) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const double bta = first ? 0.0 : ctl->beta;
   for (long long t = gtid(); t < n; t += gstride()) p[t] = first ? z[t] : T(double(z[t]) + bta * double(p[t]));
 }
@@ -661,7 +664,7 @@ __global__ void k_cg_p(long long n, T* __restrict__ p, const T* __restrict__ z, 
 template <typename T, class Post>
 __global__ void k_dot(long long n, const T* __restrict__ a, const T* __restrict__ b, RedSlot slot, Post post,
                       const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   double acc[1] = {0.0};
   for (long long t = gtid(); t < n; t += gstride()) acc[0] += double(a[t]) * double(b[t]);
   grid_reduce<1, false>(acc, slot, post);
@@ -843,7 +846,7 @@ __device__ __forceinline__ double full_weight(const GridDev& gf, const GridDev& 
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_restrict_fw(GridDev gf, GridDev gc, const T* __restrict__ rf,
                                                           TC* __restrict__ bc, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const int I = blockIdx.x * kBx + threadIdx.x;
   const int J = blockIdx.y * kBy + threadIdx.y;
   if (I >= gc.nx || J >= gc.ny) return;
@@ -880,7 +883,7 @@ inline FoldLayers fold_layers(const GridDev& g) {
 template <typename TC>
 __global__ void __launch_bounds__(256) k_restrict_fold_faces(GridDev gc, FoldLayers lay, TC* __restrict__ bc,
                                                              const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const long long ni = gc.nx - 2, nj = gc.ny - 2;
   const long long mi = ni > 2 ? ni - 2 : 0;
   const int kb = gc.dim == 3 ? 1 : 0;
@@ -937,7 +940,7 @@ __device__ __forceinline__ double ext_value(const GridDev& gc, const TC* __restr
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_prolong_add(GridDev gf, GridDev gc, const TC* __restrict__ xc,
                                                           T* __restrict__ xf, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
   int k0, k1;
@@ -1048,7 +1051,7 @@ struct FwColumn {
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_restrict_march(GridDev gf, GridDev gc, const T* __restrict__ rf,
                                                              TC* __restrict__ bc, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const int I = blockIdx.x * kBx + threadIdx.x;
   const int J = blockIdx.y * kBy + threadIdx.y;
   if (I >= gc.nx || J >= gc.ny) return;
@@ -1078,7 +1081,7 @@ __global__ void __launch_bounds__(kBx* kBy) k_restrict_march(GridDev gf, GridDev
 template <typename T, typename TC>
 __global__ void __launch_bounds__(kBx* kBy) k_prolong_march(GridDev gf, GridDev gc, const TC* __restrict__ xc,
                                                             T* __restrict__ xf, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   const int i = blockIdx.x * kBx + threadIdx.x;
   const int j = blockIdx.y * kBy + threadIdx.y;
   int k0, k1;
@@ -1309,7 +1312,7 @@ template <class Coef, typename T>
 __global__ void __launch_bounds__(kTailThreads, 1) k_tail_vcycle(const TailLevel<Coef, T>* __restrict__ lv, int nlev,
                                                                const T* __restrict__ rhs0, int pre, int post,
                                                                int coarse_iters, int fold, const Ctl* ctl) {
-  if (ctl_skip(ctl)) return;
+  if (ctl_skip_dep(ctl)) return;
   // down: smooth, residual, restrict
   for (int l = 0; l + 1 < nlev; ++l) {
     const TailLevel<Coef, T>& L = lv[l];
