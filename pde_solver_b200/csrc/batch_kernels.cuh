@@ -21,6 +21,8 @@
 // the block that restricts into it.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace pdeb {
@@ -168,7 +170,10 @@ struct FStencil {
     else
       return __ldg(k + id);
   }
+  // D: the grid dimension when the caller knows it at compile time, else 0
+  template <int D = 0>
   __device__ __forceinline__ Stencil<float> at(int i, int j, int kz, int id) const {
+    const bool d3 = D ? D == 3 : dim == 3;
     Stencil<float> s;
     if (kind == kConst) {
       s.c = c0;
@@ -187,7 +192,7 @@ struct FStencil {
       s.ym = -kym * ihy2 - dyc;
       s.yp = -kyp * ihy2 + dyc;
       float c = (kxm + kxp) * ihx2 + (kym + kyp) * ihy2;
-      if (dim == 3) {
+      if (d3) {
         const float kzm = 0.5f * (kc + kv(id - sxy)), kzp = 0.5f * (kc + kv(id + sxy));
         s.zm = -kzm * ihz2 - dzc;
         s.zp = -kzp * ihz2 + dzc;
@@ -197,8 +202,8 @@ struct FStencil {
       }
       s.c = c + e;
     }
-    if (i == 1 || i == nx - 2 || j == 1 || j == ny - 2 || (dim == 3 && (kz == 1 || kz == nz - 2)))
-      fold_faces<float>(*g, i, j, kz, s, nullptr);
+    if (i == 1 || i == nx - 2 || j == 1 || j == ny - 2 || (d3 && (kz == 1 || kz == nz - 2)))
+      fold_faces<float, D>(*g, i, j, kz, s, nullptr);
     return s;
   }
 };
@@ -408,23 +413,30 @@ __global__ void __launch_bounds__(kBThreads, 5) kb_apply_pq(const BTile* __restr
   float* __restrict__ q = m->q;
   FStencil<float> S;
   S.load(L, m->k32);
-  const int nx = S.nx, sxy = S.sxy, dim = S.dim;
-  const bool is3 = dim == 3;
+  const int nx = S.nx, sxy = S.sxy;
   double acc[1] = {0.0};
-  tile_columns(T, [&](int i, int j) {
-    int id = (T.z0 * S.ny + j) * nx + i;
-    float zm = is3 ? p[id - sxy] : 0.f;
-    float zc = p[id];
-    for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
-      const float zp = is3 ? p[id + sxy] : 0.f;
-      const Stencil<float> s = S.at(i, j, kk, id);
-      const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, dim);
-      q[id] = v;
-      acc[0] += double(zc) * double(v);
-      zm = zc;
-      zc = zp;
-    }
-  });
+  // one branch on the tile's dimension; inside, D is a constant
+  auto columns = [&](auto dc) {
+    constexpr int D = decltype(dc)::value;
+    tile_columns(T, [&](int i, int j) {
+      int id = (T.z0 * S.ny + j) * nx + i;
+      float zm = D == 3 ? p[id - sxy] : 0.f;
+      float zc = p[id];
+      for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
+        const float zp = D == 3 ? p[id + sxy] : 0.f;
+        const Stencil<float> s = S.template at<D>(i, j, kk, id);
+        const float v = s.c * zc + nb_sum<float>(s, p[id + 1], p[id - 1], p[id + nx], p[id - nx], zp, zm, D);
+        q[id] = v;
+        acc[0] += double(zc) * double(v);
+        zm = zc;
+        zc = zp;
+      }
+    });
+  };
+  if (S.dim == 3)
+    columns(std::integral_constant<int, 3>{});
+  else
+    columns(std::integral_constant<int, 2>{});
   member_reduce<1>(acc, partials, m, blockIdx.x, BPostPQ{});
 }
 
@@ -524,8 +536,8 @@ __global__ void __launch_bounds__(kBThreads, 8) kb_smooth(const BTile* __restric
       if (ra >= int(T.w)) continue;
       const int i = i0 + ra;
       const int id = j * nx + i;
-      const Stencil<float> s = S.at(i, j, 0, id);
-      x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], 0.f, 0.f, dim)) / s.c;
+      const Stencil<float> s = S.template at<2>(i, j, 0, id);
+      x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], 0.f, 0.f, 2)) / s.c;
     }
     return;
   }
@@ -541,13 +553,14 @@ __global__ void __launch_bounds__(kBThreads, 8) kb_smooth(const BTile* __restric
         }
       }
     } else {
+      // 3D here (the 2D pass returned above): the z loads are not predicated
 #pragma unroll 2
       for (int kk = T.z0 + ((i + j + T.z0 + color) & 1); kk < T.z1; kk += 2) {
         const int id = (kk * S.ny + j) * nx + i;
-        const Stencil<float> s = S.at(i, j, kk, id);
-        const float zp = is3 ? xr[id + sxy] : 0.f;
-        const float zm = is3 ? xr[id - sxy] : 0.f;
-        x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], zp, zm, dim)) / s.c;
+        const Stencil<float> s = S.template at<3>(i, j, kk, id);
+        const float zp = xr[id + sxy];
+        const float zm = xr[id - sxy];
+        x[id] = (b[id] - nb_sum<float>(s, xr[id + 1], xr[id - 1], xr[id + nx], xr[id - nx], zp, zm, 3)) / s.c;
       }
     }
   });
@@ -566,20 +579,27 @@ __global__ void __launch_bounds__(kBThreads, kBMinBlocks) kb_residual(const BTil
   float* __restrict__ r = L.r;
   FStencil<KT> S;
   S.load(L, static_cast<const KT*>(L.kh));
-  const int nx = S.nx, sxy = S.sxy, dim = S.dim;
-  const bool is3 = dim == 3;
-  tile_columns(T, [&](int i, int j) {
-    int id = (T.z0 * S.ny + j) * nx + i;
-    float zm = is3 ? x[id - sxy] : 0.f;
-    float zc = x[id];
-    for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
-      const float zp = is3 ? x[id + sxy] : 0.f;
-      const Stencil<float> s = S.at(i, j, kk, id);
-      r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, dim));
-      zm = zc;
-      zc = zp;
-    }
-  });
+  const int nx = S.nx, sxy = S.sxy;
+  // one branch on the tile's dimension; inside, D is a constant
+  auto columns = [&](auto dc) {
+    constexpr int D = decltype(dc)::value;
+    tile_columns(T, [&](int i, int j) {
+      int id = (T.z0 * S.ny + j) * nx + i;
+      float zm = D == 3 ? x[id - sxy] : 0.f;
+      float zc = x[id];
+      for (int kk = T.z0; kk < T.z1; ++kk, id += sxy) {
+        const float zp = D == 3 ? x[id + sxy] : 0.f;
+        const Stencil<float> s = S.template at<D>(i, j, kk, id);
+        r[id] = b[id] - (s.c * zc + nb_sum<float>(s, x[id + 1], x[id - 1], x[id + nx], x[id - nx], zp, zm, D));
+        zm = zc;
+        zc = zp;
+      }
+    });
+  };
+  if (S.dim == 3)
+    columns(std::integral_constant<int, 3>{});
+  else
+    columns(std::integral_constant<int, 2>{});
 }
 
 // Coarsest-level solve inside one block: `sweeps` red-black sweeps from zero
