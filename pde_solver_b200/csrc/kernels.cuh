@@ -274,7 +274,7 @@ __device__ __forceinline__ void rbgs_columns(const GridDev& g, const Coef& cf, c
 // and handed to `post` (the last two passes of a V-cycle's finest level give
 // r.z of preconditioned CG, since b is r there).
 template <class Coef, typename T, typename TB, bool ZERO = false, bool DOT = false, class Post = NoPost>
-__global__ void __launch_bounds__(kBx* kBy, ZERO ? 4 : 3)
+__global__ void __launch_bounds__(kBx* kBy, ZERO || sizeof(T) == 4 ? 4 : 3)
     k_rbgs(GridDev g, Coef cf, const TB* __restrict__ b, T* __restrict__ x, int color, const Ctl* ctl,
            RedSlot slot = RedSlot{}, Post post = Post{}) {
   if (ctl_skip_dep(ctl)) return;
