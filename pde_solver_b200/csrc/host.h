@@ -226,10 +226,15 @@ dim3 stencil_grid_full(const GridDev& g, int zchunk = 16);
 // z-chunking chosen for occupancy: about kTargetBlocks blocks, at least one
 // interior plane per thread
 dim3 stencil_grid_auto(const GridDev& g, long long target_blocks = 0);
-// launch shape of the colour passes (k_rbgs): about three waves of the three
-// blocks per SM their registers allow, measured faster than the default
-// target on every level of the 257^3 hierarchy
-inline dim3 rbgs_grid(const GridDev& g) { return stencil_grid_auto(g, 148 * 9); }
+// launch shape of the colour passes (k_rbgs): on levels larger than L2 about
+// three waves of the three blocks per SM their registers allow (faster than
+// the default target)
+inline dim3 rbgs_grid(const GridDev& g) {
+  // levels that fit in L2 (129^3 and below) launch one wave of 148 x 3 blocks:
+  // 129^3 14.6 -> 13.8 us and 65^3 4.3 -> 3.9 us per pass in a replayed graph,
+  // 257^3 solve 21.93 -> 21.8 ms, 129^3 6.2 -> 6.0 ms, 65^3 3.2 -> 3.1 ms
+  return stencil_grid_auto(g, g.n > (1LL << 22) ? 148 * 9 : 148 * 3);
+}
 // launch shape of the fused red-black sweep (64 x 8 column tiles)
 dim3 fused_grid(const GridDev& g);
 // launch shape of the marching single-pass sweep (64 x 8 interior column tiles, z chunks)
