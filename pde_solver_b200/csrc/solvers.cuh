@@ -739,8 +739,10 @@ struct Hierarchy {
     {
       ProfScope ps(ctx, "residual", l, dofs * 4.0 * sizeof(T));
       // levels that fit in L2: 148 x 6 target blocks (65^3: 4.6 -> 3.7 us per
-      // launch in a replayed graph; 129^3 unchanged)
-      launch_dep(ctx, stencil_grid_auto(L.g, L.g.n > (1LL << 22) ? 0 : 148 * 6), stencil_block(), 0,
+      // launch in a replayed graph; 129^3 unchanged); larger levels 148 x 24
+      // (12 z chunks at 257^3, an even number of planes per chunk for the
+      // two-plane trips: 108.7 -> 103.6 us per launch in the solve)
+      launch_dep(ctx, stencil_grid_auto(L.g, L.g.n > (1LL << 22) ? 148 * 24 : 148 * 6), stencil_block(), 0,
                  k_residual_folded<Coef, T, T, 0, NoPost>, L.g, L.cf, (const T*)cur, b, L.r, RedSlot{}, NoPost{},
                  ctl);
     }
