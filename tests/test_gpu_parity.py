@@ -205,3 +205,31 @@ def test_projection_256_matches_reference(ref_oracle):
     for name, a, b in (("u", ug, ur), ("v", vg, vr), ("p", pg, pr)):
         d = rel_l2(a, b)
         assert d <= 1e-10, (name, d)
+
+
+# ------------------------------------------- anisotropic constant coefficients
+
+@pytest.mark.parametrize("dims,coefs", [((33, 33, 33), (-1.0, -4.0, -0.25)), ((65, 33, 1), (-3.0, -0.5, 0.0)),
+                                        ((41, 29, 23), (-0.5, -1.0, -2.0))])
+def test_mgpcg_anisotropic_constant_matches_oracle(oracle_mod, dims, coefs):
+    # a, b, az differ by up to 16x: the smoother and the hierarchy see a
+    # strongly directional operator; both sides solve to 1e-12 relative
+    nx, ny, nz = dims
+    a, b, az = coefs
+    p = GridProblem(nx, ny, nz, a=a, b=b, az=az)
+    p.f = np.random.Generator(np.random.PCG64(nx * ny + nz)).standard_normal(p.n)
+    # Robin on min faces only: there the closure weight (beta/h)/(alpha+beta/h)
+    # stays below one and the folded operator stays definite
+    if nz == 1:
+        p.faces = [FaceBC.robin(1.0, 0.5, 0.1), FaceBC.dirichlet(0.0), FaceBC.neumann(0.2), FaceBC.dirichlet(0.3),
+                   FaceBC(), FaceBC()]
+    else:
+        p.faces = [FaceBC.robin(1.0, 1.0, 0.0), FaceBC.dirichlet(0.5), FaceBC.neumann(0.0), FaceBC.neumann(0.1),
+                   FaceBC.robin(2.0, 0.5, 0.1), FaceBC.dirichlet(0.0)]
+    opt = default_options(method=abi.MG_PCG, tol=1e-12, tol_mode=abi.TOL_RELATIVE, max_iter=400)
+    got, rep = solver.solve(p, opt)
+    st, ref, rrep = oracle_mod.rs_solve(p, opt)
+    assert st == 0 and rep.status == abi.OK
+    assert rep.rel_residual <= 1e-12
+    assert abs(rep.iterations - rrep.iterations) <= 1
+    assert rel_l2(got, ref) <= 1e-9
