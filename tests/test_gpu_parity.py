@@ -136,14 +136,16 @@ NONLINEAR = [
 ]
 
 
-@pytest.mark.parametrize("dims", [(21, 19, 1), (11, 10, 9), (70, 66, 1), (24, 22, 20)])
+# every term kind on the small grids, two kinds on the larger ones
+NONLINEAR_CASES = [(dims, name, terms) for dims in [(21, 19, 1), (11, 10, 9), (70, 66, 1), (24, 22, 20)]
+                   for name, terms in NONLINEAR if dims[0] * dims[1] * dims[2] <= 2000 or name in ("u2", "sin")]
+
+
 @pytest.mark.parametrize("method,omega", [(abi.JACOBI, 1.0), (abi.GAUSS_SEIDEL, 1.0), (abi.SOR, 1.5)])
-@pytest.mark.parametrize("name,terms", NONLINEAR)
+@pytest.mark.parametrize("dims,name,terms", NONLINEAR_CASES)
 def test_relaxation_nonlinear_terms_match_reference(ref_oracle, dims, method, omega, name, terms):
     # sum(coeff * g(u_old)) inside every relaxation update (EvalNonlinear,
     # relaxation.cpp:27-45,217-218,476-477; solver.cpp:884-885)
-    if dims[0] * dims[1] * dims[2] > 2000 and name not in ("u2", "sin"):
-        pytest.skip("two term kinds per larger size")
     _nonlinear_case(ref_oracle, dims, method, omega, terms, 1e-11)
 
 
