@@ -113,6 +113,18 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation and the first query) is
+        # its heaviest part: wait for the first sample before the caller's
+        # timed region begins (at most 5 s)
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is not None:
